@@ -1,0 +1,358 @@
+"""Benchmark of the TLS search on B200: light curves per second.
+
+Default workload (one step = one full search of one light curve, as
+``gtls(t, y, dy).power()`` runs it: main pass over every trial period, SDE
+spectra, FP64 re-search of the 200 candidates and 5 harmonics, best-period
+finish):
+
+  long-baseline FP64 search -- 70,000 samples at 29.4-min cadence over
+  ~1,470 d with 17 gaps, per-sample sigma U(50, 500) ppm + AR(1) red noise,
+  one 490 ppm transit at P = 289.9 d; Ofir grid 0.5-735 d at oversampling 3
+  (187,870 periods), 50 durations.  Seeded synthetic data.
+
+``value`` is device-timed with the inputs resident in HBM; ``e2e`` times the
+public API from host arrays (host->device copies and result readback inside
+the timed region).  Under torchrun every rank searches its own light curve
+(independent replicas, no collective in the data path; weak scaling) and
+``value`` is the total over ranks.  ``--impl reference`` times the
+reference's own kernel code compiled for the host CPU (oracle/_ref, all
+cores) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "light curves/s (long-baseline TLS search, 70k samples, 187,870 periods x 50 durations)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def durations_step_for(periods, n, want):
+    """duration_grid_step giving exactly ``want`` durations."""
+    from gtls_b200.grid import duration_grid
+    lo, hi = 1.0001, 3.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        c = len(duration_grid(periods, shortest=1 / n, log_step=mid))
+        if c > want:
+            lo = mid
+        elif c < want:
+            hi = mid
+        else:
+            return mid
+    raise RuntimeError("no duration step gives %d durations" % want)
+
+
+def workload(name, rank=0):
+    from gtls_b200 import synthetic, validate as V
+    if name == "cfg2":
+        t, y, dy, truth = synthetic.light_curve_cfg2(seed=rank)
+        kw = dict(period_min=0.5, period_max=735.0, oversampling_factor=3)
+        n_dur = 50
+        desc = "cfg2: 70,000 samples, 29.4-min cadence, ~1,470 d, 17 gaps; Ofir 0.5-735 d osf 3; 50 durations"
+    else:
+        t, y, dy, truth = synthetic.light_curve_cfg1(seed=rank)
+        kw = dict(period_min=0.5, period_max=13.7, oversampling_factor=3)
+        n_dur = None
+        desc = "cfg1: 19,728 samples, 2-min cadence, 27.4 d + 1 d gap; Ofir 0.5-13.7 d osf 3; default durations"
+    t, y, dy = V.validate_inputs(t, y, dy)
+    return t, y, dy, truth, kw, n_dur, desc
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(t, y, dy, periods, kw, step, batch_hint, budget_s=15.0, seed=0):
+    """Time the reference's kernels (compiled for the CPU, all host cores) on a
+    sample of the workload and extrapolate to one full search."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_replay as RR
+    import tls_oracle as O
+    from gtls_b200 import grid as G, template
+    if not RR.available("r64_skip8"):
+        return None
+    durs = G.duration_grid(periods, shortest=1 / len(t), log_step=step)
+    mw = int(np.max(durs) * len(y))
+    mw += mw % 2
+    ov, lc = template.get_cache(durs, mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+    widths, os_, _, tm, maxd = template.device_templates(lc, ov)
+    rb = RR.RefKernelBackend("r64", 8)
+    rng = np.random.default_rng(seed)
+    span = t.max() - t.min()
+    wmin, wmax = O.duration_ranges(periods, span, len(t))
+    masks = O.duration_masks(wmin, wmax, widths)
+    unions = O.batch_unions(masks, batch_hint)
+    main_t, main_n, all_t, all_n = 0.0, 0, 0.0, 0
+    t_begin = time.time()
+    order = rng.permutation(len(periods))
+    i = 0
+    while time.time() - t_begin < budget_s * 0.75 and i < len(order):
+        p = order[i]
+        sel = unions[p // batch_hint]
+        a = time.time()
+        rb.main_pass(t, y, dy, periods[p], widths[sel], tm[sel], os_[sel], maxd, 1e-5, 8)
+        main_t += time.time() - a
+        main_n += 1
+        i += 1
+    while time.time() - t_begin < budget_s and all_n < 3:
+        p = order[i + all_n]
+        sel = unions[p // batch_hint]
+        a = time.time()
+        rb.noskip_pass(t, y, dy, periods[p], widths[sel], tm[sel], os_[sel], maxd, 1e-5)
+        all_t += time.time() - a
+        all_n += 1
+    per_main = main_t / max(main_n, 1)
+    per_all = all_t / max(all_n, 1) if all_n else per_main * 8
+    total = per_main * len(periods) + per_all * 206
+    return dict(value=1.0 / total, unit="light curves/s", cores=os.cpu_count(), kind="reference",
+                sample="%d main-pass periods + %d all-starts periods of the workload through the reference's "
+                       "kernels compiled for the CPU (oracle/_ref, OpenMP, %d threads), extrapolated to %d + 206 "
+                       "periods" % (main_n, all_n, os.cpu_count(), len(periods)),
+                seconds_per_curve=total)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from gtls_b200 import grid as G
+        t, y, dy, truth, kw, n_dur, desc = workload(args.workload)
+        a3, c, npts, _ = G.ofir_coefficients(1.0, 1.0, t.max() - t.min(), kw["oversampling_factor"], 2)
+        X = np.arange(npts) + 1.0
+        periods = 1 / (a3 * X + c) ** 3 / 86400
+        periods = np.sort(periods[(periods > kw["period_min"]) & (periods <= kw["period_max"])])
+        step = durations_step_for(periods, len(t), n_dur) if n_dur else 1.1
+        steps = []
+        res = None
+        for i in range(args.warmup + args.steps):
+            r = cpu_reference(t, y, dy, periods, kw, step, max(1, len(periods) // 30),
+                              budget_s=4.0 if i < args.warmup else 12.0, seed=i)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+                return 0
+            if i >= args.warmup:
+                steps.append(r["seconds_per_curve"])
+                res = r
+        v = 1.0 / statistics.median(steps)
+        line = {"metric": METRIC, "value": v, "unit": "light curves/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(steps),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": desc, "periods": len(periods), "durations": n_dur},
+                "cpu_baseline": dict(value=v, unit="light curves/s", cores=res["cores"], kind="reference",
+                                     sample=res["sample"]),
+                "e2e": {"value": v, "unit": "light curves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    from gtls_b200 import _lib, core, grid as G, gtls
+    from gtls_b200.template import get_cache
+
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    device = torch.cuda.current_device()
+    t, y, dy, truth, kw, n_dur, desc = workload(args.workload, rank)
+    periods = np.sort(G.period_grid(1.0, 1.0, t.max() - t.min(), kw["period_min"], kw["period_max"],
+                                    kw["oversampling_factor"], 2, device=device, ascending=True))
+    step = durations_step_for(periods, len(t), n_dur) if n_dur else 1.1
+    durations = G.duration_grid(periods, shortest=1 / len(t), log_step=step)
+    mw = int(np.max(durations) * len(y))
+    mw += mw % 2
+    ov, lc = get_cache(durations, mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+    cur = core.CurveOnDevice(t, y, dy, lc, ov, device=device)
+    periods_dev = torch.from_numpy(periods).to(cur.dev)
+    free = torch.cuda.mem_get_info(device)[0]
+    batch = core.reference_batch_size(len(periods), cur.n, cur.maxd, len(cur.widths), free)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cur.dev)  # > 126 MB L2
+
+    def one_step(timing=None):
+        return core.run_search(cur, periods, periods_dev, t, y, dy, 1e-5, 0.125, kw["oversampling_factor"],
+                               precision=args.precision, batch_periods=batch, timing=timing)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = _lib.launch_count(device)
+    timings = []
+    step_ms = []
+    with Clocks(device) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            tm = _lib.Timing()
+            e0.record()
+            out = one_step(tm)
+            e1.record()
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            timings.append(tm.as_dict())
+    launches = _lib.launch_count(device) - launches0
+    total_ms = sum(step_ms)
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=cur.dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = world * 1000.0 / ms_per_step
+
+    # end to end through the public API from host arrays
+    model = gtls(t, y, dy, verbose=False)
+    api_kw = dict(period_min=kw["period_min"], period_max=kw["period_max"], batch_periods=batch,
+                  duration_grid_step=step, oversampling_factor=kw["oversampling_factor"], precision=args.precision,
+                  GPUDeviceID=device)
+    model.power(**api_kw)
+    torch.cuda.synchronize()
+    core.TRANSFER.update(h2d=0, d2h=0)
+    e2e_ms = []
+    for _ in range(max(1, args.steps // 2)):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        model = gtls(t, y, dy, verbose=False)
+        model.power(**api_kw)
+        torch.cuda.synchronize()
+        e2e_ms.append(1000.0 * (time.perf_counter() - a))
+    h2d = core.TRANSFER["h2d"] // len(e2e_ms)
+    d2h = core.TRANSFER["d2h"] // len(e2e_ms)
+    e2e_ms_step = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        tt = torch.tensor([e2e_ms_step], dtype=torch.float64, device=cur.dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms_step = float(tt.item())
+
+    # roofline of the dominant kernel (chi2), from the library's CUDA events
+    chi2_ms = statistics.mean(tm["chi2_ms"] for tm in timings)
+    chunks = timings[0]["chunks"]
+    n = len(t)
+    bytes_per_period = 24 * n   # t, y, w in FP64 per (curve, period)
+    achieved_gbs = bytes_per_period * len(periods) / (chi2_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        hbm_peak, peak_src = 6650.0, "fallback"
+    flops = 2.0 * statistics.mean(tm["chi2_fma"] for tm in timings)
+    pipe_tflops = flops / (chi2_ms * 1e-3) / 1e12
+    pipe_peak = 148 * (64 if args.precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "light curves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": desc, "periods": len(periods), "durations": len(cur.widths), "samples": n,
+                   "batch_periods": batch, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed (256 MB write) before every timed step; per-period scratch > L2",
+                   "precision": args.precision},
+        "e2e": {"value": world * 1000.0 / e2e_ms_step, "unit": "light curves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step},
+        "gpu_launches": int(launches // args.steps),
+        "roofline": {"bound": "hbm", "kernel": "chi2_kernel", "achieved": achieved_gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": None,
+                     "peak_source": peak_src, "launches_per_step": chunks,
+                     "avg_launch_ms": chi2_ms / max(chunks, 1),
+                     "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64"},
+        "pipe": {"unit": "TFLOP/s", "fp_pipe": "fp64" if args.precision == "fp64" else "fp32",
+                 "achieved": pipe_tflops, "nominal_peak": pipe_peak, "frac": pipe_tflops / pipe_peak,
+                 "flops": "2 per (start, template sample) for B and for C"},
+        "stages_ms": {k: statistics.mean(tm[k] for tm in timings) for k in
+                      ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
+        "result": {"period": float(out[1]), "true_period": truth["period"], "SDE": float(out[7])},
+    }
+    if rank == 0:
+        with Clocks(device) as _:
+            pass
+        line["clocks"] = clk.summary()
+        if not args.no_cpu_baseline:
+            cb = cpu_reference(t, y, dy, periods, kw, step, batch)
+            if cb is not None:
+                cb.pop("seconds_per_curve")
+                line["cpu_baseline"] = cb
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,249 @@
+"""ctypes binding of ``libgtls_b200.so`` (declared in ``include/gtls_b200.h``).
+
+The library is loaded from the package directory.  There is no fallback:
+if the library is missing or no CUDA device is present every call raises.
+Device buffers are torch tensors (torch is used for device memory and
+streams only); calls run on torch's current CUDA stream.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgtls_b200.so")
+
+ABI_VERSION = 1
+GTLS_FP64, GTLS_FP32 = 0, 1
+GTLS_PASS_MAIN, GTLS_PASS_ALL = 0, 1
+MAX_DURATIONS = 1024
+
+_lib = None
+_lock = threading.Lock()
+_ctxs = {}
+
+# bytes copied host->device and device->host by this package (accounting)
+TRANSFER = {"h2d": 0, "d2h": 0}
+
+
+def h2d(torch, arr, dev):
+    arr = np.ascontiguousarray(arr)
+    TRANSFER["h2d"] += arr.nbytes
+    return torch.from_numpy(arr).to(dev)
+
+
+def d2h(tensor):
+    TRANSFER["d2h"] += tensor.numel() * tensor.element_size()
+    return tensor.cpu().numpy()
+
+
+class GtlsError(RuntimeError):
+    """A gtls_* C-ABI call returned a non-zero status."""
+
+
+class Timing(ctypes.Structure):
+    """Mirror of ``gtls_timing``."""
+    _fields_ = [
+        ("chunks", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("setup_ms", ctypes.c_double),
+        ("prepare_ms", ctypes.c_double),
+        ("chi2_ms", ctypes.c_double),
+        ("finish_ms", ctypes.c_double),
+        ("chi2_starts", ctypes.c_int64),
+        ("chi2_fma", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class SearchDesc(ctypes.Structure):
+    """Mirror of ``gtls_search_desc``."""
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("pass_", ctypes.c_int32),
+        ("n", ctypes.c_int32),
+        ("t", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("dy", ctypes.c_void_p),
+        ("n_periods", ctypes.c_int64),
+        ("periods", ctypes.c_void_p),
+        ("n_durations", ctypes.c_int32),
+        ("max_width", ctypes.c_int32),
+        ("widths", ctypes.c_void_p),
+        ("overshoot", ctypes.c_void_p),
+        ("templates", ctypes.c_void_p),
+        ("depth_min", ctypes.c_double),
+        ("skip_point", ctypes.c_int32),
+        ("batch", ctypes.c_int32),
+        ("span", ctypes.c_float),
+        ("reserved", ctypes.c_int32),
+        ("chi2_out", ctypes.c_void_p),
+        ("loc_out", ctypes.c_void_p),
+        ("timing", ctypes.c_void_p),
+    ]
+
+
+EXPORTS = {
+    "gtls_ctx_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "gtls_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "gtls_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "gtls_abi_version": ([], ctypes.c_int),
+    "gtls_launch_count": ([ctypes.c_void_p], ctypes.c_int64),
+    "gtls_period_grid": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
+                          ctypes.c_double, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p],
+                         ctypes.c_int),
+    "gtls_duration_ranges": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_int32,
+                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "gtls_search": ([ctypes.c_void_p, ctypes.POINTER(SearchDesc), ctypes.c_void_p], ctypes.c_int),
+    "gtls_spectra": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
+}
+
+
+def load():
+    """Load the library and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise GtlsError(LIB_PATH + " is missing: build it with `python -m gtls_b200.build`")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (args, res) in EXPORTS.items():
+                fn = getattr(lib, name)
+                fn.argtypes = args
+                fn.restype = res
+            if lib.gtls_abi_version() != ABI_VERSION:
+                raise GtlsError("libgtls_b200.so ABI version mismatch")
+            _lib = lib
+    return _lib
+
+
+def context(device=0):
+    """The (cached) gtls context of CUDA device ``device``."""
+    lib = load()
+    with _lock:
+        c = _ctxs.get(device)
+        if c is None:
+            h = ctypes.c_void_p()
+            rc = lib.gtls_ctx_create(device, ctypes.byref(h))
+            if rc != 0:
+                raise GtlsError("gtls_ctx_create failed (%d): %s" % (rc, lib.gtls_last_error(None).decode()))
+            c = _ctxs[device] = h
+    return c
+
+
+def _check(rc, ctx, what):
+    if rc != 0:
+        msg = load().gtls_last_error(ctx).decode(errors="replace")
+        raise GtlsError("%s failed (%d): %s" % (what, rc, msg))
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise GtlsError("gtls_b200 needs a CUDA device (none is visible)")
+    return torch
+
+
+def _stream(torch, device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def period_grid(a_over_3, c, n_points, period_min, period_max, device=0):
+    """Ascending Ofir periods from the device (gtls_period_grid)."""
+    torch = _torch()
+    ctx = context(device)
+    out = torch.empty(max(int(n_points), 1), dtype=torch.float64, device="cuda:%d" % device)
+    cnt = ctypes.c_int64()
+    pmax = float(period_max) if np.isfinite(period_max) else float("inf")
+    rc = load().gtls_period_grid(ctx, float(a_over_3), float(c), int(n_points), float(period_min), pmax,
+                                 _ptr(out), ctypes.byref(cnt), _stream(torch, device))
+    _check(rc, ctx, "gtls_period_grid")
+    return d2h(out[: cnt.value])
+
+
+def duration_ranges(periods, span, n_samples, device=0):
+    """(wmin, wmax) per period (gtls_duration_ranges), as numpy int arrays."""
+    torch = _torch()
+    ctx = context(device)
+    p = h2d(torch, np.asarray(periods, dtype=np.float64), "cuda:%d" % device)
+    wmin = torch.empty(len(p), dtype=torch.int32, device=p.device)
+    wmax = torch.empty_like(wmin)
+    rc = load().gtls_duration_ranges(ctx, _ptr(p), len(p), float(np.float32(span)), int(n_samples), _ptr(wmin),
+                                     _ptr(wmax), _stream(torch, device))
+    _check(rc, ctx, "gtls_duration_ranges")
+    return d2h(wmin).astype(np.int64), d2h(wmax).astype(np.int64)
+
+
+def launch_count(device=0):
+    """Kernels launched so far through the device's context."""
+    return int(load().gtls_launch_count(context(device)))
+
+
+def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precision, device=0,
+           want_loc=True, timing=None):
+    """Run gtls_search for one curve.
+
+    ``curve``: dict of device tensors t, y, dy (float64) and ``span`` (float).
+    ``tables``: dict of device tensors widths (int32), overshoot (float64),
+    templates (float64, D x max_width) and int ``max_width``.
+    ``periods``: device float64 tensor.  ``timing``: an optional ``Timing``
+    filled with CUDA-event stage times.  Returns (chi2, loc) device tensors.
+    """
+    torch = _torch()
+    ctx = context(device)
+    n_periods = int(periods.numel())
+    chi2 = torch.empty(n_periods, dtype=torch.float64, device=periods.device)
+    loc = torch.empty(n_periods, dtype=torch.int64, device=periods.device) if want_loc else None
+    d = SearchDesc()
+    d.abi_version = ABI_VERSION
+    d.precision = GTLS_FP32 if precision == "fp32" else GTLS_FP64
+    d.pass_ = pass_
+    d.n = int(curve["t"].numel())
+    d.t = curve["t"].data_ptr()
+    d.y = curve["y"].data_ptr()
+    d.dy = curve["dy"].data_ptr()
+    d.n_periods = n_periods
+    d.periods = periods.data_ptr()
+    d.n_durations = int(tables["widths"].numel())
+    d.max_width = int(tables["max_width"])
+    d.widths = tables["widths"].data_ptr()
+    d.overshoot = tables["overshoot"].data_ptr()
+    d.templates = tables["templates"].data_ptr()
+    d.depth_min = float(depth_min)
+    d.skip_point = int(skip_point)
+    d.batch = int(batch)
+    d.span = float(curve["span"])
+    d.chi2_out = chi2.data_ptr()
+    d.loc_out = loc.data_ptr() if loc is not None else None
+    d.timing = ctypes.addressof(timing) if timing is not None else None
+    rc = load().gtls_search(ctx, ctypes.byref(d), _stream(torch, device))
+    _check(rc, ctx, "gtls_search")
+    return chi2, loc
+
+
+def spectra(chi2, mask, oversampling_factor, device=0):
+    """gtls_spectra on a device chi2 tensor; returns (SR, power_raw, power, SDE_raw, SDE)."""
+    torch = _torch()
+    ctx = context(device)
+    n = int(chi2.numel())
+    sr = torch.empty_like(chi2)
+    praw = torch.empty_like(chi2)
+    power = torch.empty_like(chi2)
+    sde_raw = ctypes.c_double()
+    sde = ctypes.c_double()
+    rc = load().gtls_spectra(ctx, _ptr(chi2), _ptr(mask), n, float(oversampling_factor), _ptr(sr), _ptr(praw),
+                             _ptr(power), ctypes.byref(sde_raw), ctypes.byref(sde), _stream(torch, device))
+    _check(rc, ctx, "gtls_spectra")
+    return sr, praw, power, sde_raw.value, sde.value

@@ -1,0 +1,81 @@
+"""User API: ``gtls(t, y, dy).power(**kwargs)`` (the reference's ``src/gputls/main.py``).
+
+Same constructor, same ``power()`` keywords (constants.VALID_PARAMETERS) and
+the same return: a ``gtlsResult`` or, with ``fast=True``, ``(periods, power)``.
+The search runs on one GPU (``GPUDeviceID``); ``GPUDeviceIDs`` with more than
+one entry is accepted and runs on the first device (multi-GPU sharding of a
+single light curve is not part of this implementation).
+Extra keywords: ``precision`` ("fp64" plain FP64 search, default; "fp32" FP32
+chi2 with compensated prefix sums and FP64 re-search of the candidates) and
+``batch_periods`` (periods per duration-union batch; default: the reference's
+free-memory formula, core.py:620-628).
+"""
+import warnings
+
+import numpy as np
+
+from . import constants, core
+from .grid import duration_grid, period_grid
+from .results import gtlsResult
+from .template import get_cache
+from .validate import validate_args, validate_inputs
+
+
+class gtls(object):
+    """Transit least squares of limb-darkened transit models on a B200."""
+
+    def __init__(self, t, y, dy=None, verbose=True):
+        self.t, self.y, self.dy = validate_inputs(t, y, dy)
+        self.verbose = verbose
+
+    def _grids(self):
+        if len(self.periods) == 0:
+            periods = period_grid(R_star=self.R_star, M_star=self.M_star,
+                                  time_span=np.max(self.t) - np.min(self.t), period_min=self.period_min,
+                                  period_max=self.period_max, oversampling_factor=self.oversampling_factor,
+                                  n_transits_min=self.n_transits_min, device=self.GPUDeviceID)
+        else:
+            periods = np.asarray(self.periods, dtype=np.float64)
+        return periods
+
+    def power(self, **kwargs):
+        """Run the search; see the module docstring for the keywords."""
+        self, kwargs = validate_args(self, kwargs)
+        if self.GPUDeviceIDs is not None and len(self.GPUDeviceIDs) > 0:
+            if len(self.GPUDeviceIDs) > 1:
+                warnings.warn("GPUDeviceIDs: the search runs on device %d only" % self.GPUDeviceIDs[0])
+            self.GPUDeviceID = self.GPUDeviceIDs[0]
+        if self.verbose:
+            print(constants.BANNER)
+        periods = self._grids()
+        durations = duration_grid(periods, shortest=1 / len(self.t), log_step=self.duration_grid_step)
+        maxwidth = int(np.max(durations) * np.size(self.y))
+        if maxwidth % 2 != 0:
+            maxwidth = maxwidth + 1
+        self.maxwidth_in_samples = maxwidth
+        self.lc_cache_overview, self.lc_arr = get_cache(
+            durations=durations, maxwidth_in_samples=maxwidth, per=self.per, rp=self.rp, a=self.a,
+            inc=self.inc, ecc=self.ecc, w=self.w, u=self.u, limb_dark=self.limb_dark, verbose=self.verbose)
+        if self.verbose:
+            print("Searching " + str(len(self.y)) + " data points, " + str(len(periods)) + " periods from "
+                  + str(round(min(periods), 3)) + " to " + str(round(max(periods), 3)) + " days")
+        periods = np.sort(periods)
+        out = core.search_multi_periods(
+            periods=periods, t=self.t, y=self.y, dy=self.dy, transit_depth_min=self.transit_depth_min,
+            lc_arr=self.lc_arr, lc_cache_overview=self.lc_cache_overview, T0_fit_margin=self.T0_fit_margin,
+            oversampling_factor=self.oversampling_factor, verbose=self.verbose, GPUDeviceID=self.GPUDeviceID,
+            fast=self.fast, precision=self.precision, batch_periods=self.batch_periods)
+        if self.fast:
+            return out
+        (self.periods, self.period, self.rawDuration, durationPoints, self.duration, self.Depth, self.bestT0,
+         SDE, chi2, self.transitTimes, power, snr, snrPink, snrFit, snrFitPink, raw_power, raw_chi2,
+         cand_idx, cand_p, diag) = out
+        self.rawDurations = durations
+        return gtlsResult(self.periods, self.period, self.rawDuration, durationPoints, durations, self.duration,
+                          self.Depth, self.bestT0, SDE, chi2, self.transitTimes, power, snr, snrPink, snrFit,
+                          snrFitPink, raw_power, raw_chi2, cand_idx, cand_p, diag)
+
+    def periodogram(self, **kwargs):
+        """The trial periods power() would search (main.py:186-205)."""
+        self, kwargs = validate_args(self, kwargs)
+        return self._grids()

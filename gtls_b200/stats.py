@@ -1,0 +1,108 @@
+"""Host statistics of the best period (NumPy, as the reference runs them).
+
+Restated from the reference's ``src/gputls/stats.py``: ``all_transit_times``
+(:233-250), ``calcDurationDays`` (:252-275), ``intransit_stats`` (:351-424),
+``pink_noise`` (:426-431), ``snr_stats`` (:433-488), and
+``helpers.transit_mask`` (helpers.py:62-65).  These are O(N) host steps after
+the search; ``pink_noise`` is vectorised (the reference loops in Python).
+"""
+import numpy as np
+
+
+def transit_mask(t, period, duration, T0):
+    return np.abs((t - T0 + 0.5 * period) % period - 0.5 * period) < 0.5 * duration
+
+
+def all_transit_times(T0, t, period):
+    transit_times = [T0 + period] if T0 < min(t) else [T0]
+    prev = transit_times[0]
+    end = np.min(t) + (np.max(t) - np.min(t))
+    while True:
+        nxt = prev + period
+        if nxt < end:
+            transit_times.append(nxt)
+            prev = nxt
+        else:
+            break
+    return transit_times
+
+
+def calc_duration_days(times, period, start_t0, raw_duration):
+    """Duration in days from the phase-sorted samples after the nearest-to-centre one.
+
+    The end index is clamped to the last sample (the reference indexes past the
+    array and raises IndexError when the duration reaches beyond it).
+    """
+    t0c = start_t0 + period / 2
+    phases = (times - t0c) / period - np.floor((times - t0c) / period)
+    ps = phases[np.argsort(phases)]
+    start = int(np.abs(ps - 0.5).argmin())
+    end = min(start + int(np.array(raw_duration) * len(times)), len(times) - 1)
+    return (ps[end] - 0.5) * period
+
+
+def intransit_stats(t, y, transit_times, transit_duration_in_days):
+    odd = []
+    even = []
+    per_transit_count = np.zeros(len(transit_times))
+    transit_depths = np.zeros(len(transit_times))
+    uncert = np.zeros(len(transit_times))
+    for i, mid in enumerate(transit_times):
+        tmin = mid - 0.5 * transit_duration_in_days
+        tmax = mid + 0.5 * transit_duration_in_days
+        if np.isnan(tmin) or np.isnan(tmax):
+            flux = np.array([])
+            mean_flux = np.nan
+        else:
+            flux = y[np.logical_and(t > tmin, t < tmax)]
+            mean_flux = np.mean(flux) if len(flux) > 0 else np.nan
+        transit_depths[i] = mean_flux
+        uncert[i] = np.std(flux) / np.sqrt(flux.size) if flux.size > 0 else np.nan
+        per_transit_count[i] = flux.size
+        (even if i % 2 == 0 else odd).append(flux)
+    odd = np.concatenate(odd) if odd else np.array([])
+    even = np.concatenate(even) if even else np.array([])
+    d_odd = np.mean(odd) if len(odd) else np.nan
+    d_even = np.mean(even) if len(even) else np.nan
+    s_odd = np.std(odd) / len(odd) ** 0.5 if len(odd) else np.nan
+    s_even = np.std(even) / len(even) ** 0.5 if len(even) else np.nan
+    return d_odd, d_even, s_odd, s_even, odd, even, per_transit_count, transit_depths, uncert
+
+
+def pink_noise(data, width):
+    """Mean standard deviation of all windows of ``width`` samples, / sqrt(width)."""
+    n = len(data) - width + 1
+    if width < 1 or n < 1:
+        raise ValueError("pink_noise window does not fit the data")
+    win = np.lib.stride_tricks.sliding_window_view(np.asarray(data, dtype=float), width)
+    return np.sum(np.std(win, axis=1)) / (n * width ** 0.5)
+
+
+def snr_stats(t, y, period, duration, T0, transit_times, transit_duration_in_days, per_transit_count):
+    snr_per_transit = np.zeros(len(transit_times))
+    snr_pink_per_transit = np.zeros(len(transit_times))
+    intransit = transit_mask(t, period, 2 * duration, T0)
+    flux_ootr = y[~intransit]
+    try:
+        pinknoise = pink_noise(flux_ootr, int(np.mean(per_transit_count)))
+    except Exception:
+        pinknoise = np.nan
+    std = np.std(flux_ootr) if len(flux_ootr) > 0 else np.nan
+    for i, mid in enumerate(transit_times):
+        tmin = mid - 0.5 * transit_duration_in_days
+        tmax = mid + 0.5 * transit_duration_in_days
+        if np.isnan(tmin) or np.isnan(tmax):
+            flux = np.array([])
+            mean_flux = np.nan
+        else:
+            flux = y[np.logical_and(t > tmin, t < tmax)]
+            mean_flux = np.mean(flux) if len(flux) > 0 else np.nan
+        pts = flux.size
+        with np.errstate(divide="ignore", invalid="ignore"):
+            snr_pink_per_transit[i] = (1 - mean_flux) / pinknoise
+            if pts > 0 and not np.isnan(std):
+                snr_per_transit[i] = (1 - mean_flux) / (std / pts ** 0.5)
+            else:
+                snr_per_transit[i] = 0
+                snr_pink_per_transit[i] = 0
+    return snr_per_transit, snr_pink_per_transit

@@ -1,0 +1,161 @@
+/*
+ * gtls_b200 -- C-ABI of the B200-native Transit Least Squares search.
+ *
+ * Every buffer argument is a DEVICE pointer owned by the caller unless the
+ * comment says "host".  Every call is asynchronous on the given stream
+ * (cudaStream_t passed as void*; NULL = the legacy default stream) except
+ * where it says it synchronises.  Every call returns 0 on success and a
+ * GTLS_E_* code otherwise; gtls_last_error() gives the message.  No C++
+ * exception crosses this interface.  A context belongs to one device and
+ * must not be used from two host threads at once.
+ *
+ * These entry points replace the reference's cupy RawModule kernel launches
+ * and their host glue (reference file:line given per function).
+ */
+#ifndef GTLS_B200_H
+#define GTLS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GTLS_ABI_VERSION 1
+
+enum gtls_status {
+  GTLS_OK = 0,
+  GTLS_E_INVALID = 1,   /* bad argument (size, pointer, mode)            */
+  GTLS_E_CUDA = 2,      /* a CUDA runtime call failed                    */
+  GTLS_E_NOMEM = 3,     /* scratch allocation failed                     */
+  GTLS_E_RANGE = 4,     /* input outside the supported range             */
+  GTLS_E_DEVICE = 5     /* a kernel reported an error through its status word */
+};
+
+enum gtls_precision {
+  GTLS_FP64 = 0,        /* plain FP64 chi2                                */
+  GTLS_FP32 = 1         /* FP32 chi2, compensated FP32 prefix sums, FP64 baseline */
+};
+
+enum gtls_pass {
+  GTLS_PASS_MAIN = 0,   /* starts k with k % skip == 0 (GPUFun.py:402,409) */
+  GTLS_PASS_ALL = 1     /* every start (GPUFun.py:646-695, 819-873)         */
+};
+
+typedef struct gtls_ctx gtls_ctx;
+
+/* Create / destroy a context on CUDA device `device`.  The context owns the
+ * scratch arena the searches use. */
+int gtls_ctx_create(int device, gtls_ctx** out);
+int gtls_ctx_destroy(gtls_ctx* ctx);
+
+/* Message of the last failed call on this context (or of the last failed
+ * gtls_ctx_create when ctx is NULL).  Never NULL. */
+const char* gtls_last_error(const gtls_ctx* ctx);
+
+/* ABI version compiled into the library (GTLS_ABI_VERSION). */
+int gtls_abi_version(void);
+
+/* Number of kernels this context has launched since it was created
+ * (no counterpart in the reference; used to account for device work). */
+int64_t gtls_launch_count(const gtls_ctx* ctx);
+
+/*
+ * Ofir-optimal period grid, evaluated on the device.
+ * Replaces the per-point part of grid.period_grid (grid.py:126-137):
+ * P(X) = 1 / (a_over_3 * X + c)^3 / 86400 for X = 1..n_points, keeping
+ * period_min < P <= period_max.  Writes the kept periods in ASCENDING order
+ * (main.py:75 sorts them) to periods_out (capacity n_points) and their count
+ * to *count_out (host).  Synchronises the stream.
+ */
+int gtls_period_grid(gtls_ctx* ctx, double a_over_3, double c, int64_t n_points,
+                     double period_min, double period_max, double* periods_out,
+                     int64_t* count_out, void* stream);
+
+/*
+ * Per-period duration range in samples.  Replaces the durationsGrid kernel
+ * (GPUFun.py:47-86): wmin = floor(min(T14min/P, 0.15) * n_samples),
+ * wmax = ceil(min(T14max/P, 0.15) * n_samples * (span/P + 1)/(span/P)),
+ * with the time span given as float (as _worker.py:107 passes it).
+ */
+int gtls_duration_ranges(gtls_ctx* ctx, const double* periods, int64_t n_periods, float span,
+                         int32_t n_samples, int32_t* wmin, int32_t* wmax, void* stream);
+
+/* Stage times of one gtls_search call, measured with CUDA events on the
+ * call's stream (filled only when gtls_search_desc.timing is non-NULL; the
+ * call then synchronises the stream before returning). */
+typedef struct gtls_timing {
+  int32_t chunks;             /* period chunks (one prepare + chi2 launch each) */
+  int32_t reserved;
+  double setup_ms;            /* curve set-up, duration ranges, unions, template rows */
+  double prepare_ms;          /* fold + ranking + gather + prefix, all chunks   */
+  double chi2_ms;             /* chi2 kernel, all chunks                        */
+  double finish_ms;           /* per-period minimum, all chunks                 */
+  int64_t chi2_starts;        /* (duration, start) evaluations done by the chi2 kernel */
+  int64_t chi2_fma;           /* multiply-adds of B and C issued by the chi2 kernel */
+} gtls_timing;
+
+/*
+ * One light curve's search over a list of trial periods.  Replaces the batch
+ * loop of core.search_multi_periods (core.py:691-875), of
+ * core.search_multi_periods_again (core.py:1081-1237) and the chi2 part of
+ * core.search_single_periods (core.py:1292-1418).
+ *
+ * For every period p the durations searched are those d with
+ * wmin(q) <= widths[d] <= wmax(q) for at least one period q of p's batch
+ * (consecutive groups of `batch` periods; the reference's per-batch union,
+ * core.py:693-716).  chi2_out[p] is the minimum over (duration, start) of
+ *   - the template chi2 of the window of `widths[d]` folded samples starting
+ *     at k, when the window's mean depth exceeds depth_min and (pass MAIN)
+ *     k % skip(d) == 0 with skip(d) = widths[d] / skip_point if
+ *     widths[d] > skip_point else 1;
+ *   - n (the sample count) otherwise (GPUFun.py:407,437).
+ * loc_out[p] = d_pos * n + k of the first minimum, d_pos counting the
+ * batch's durations in ascending width.  A batch with no duration gets NaN
+ * and loc -1 (core.py:722-729).
+ */
+typedef struct gtls_search_desc {
+  int32_t abi_version;        /* GTLS_ABI_VERSION                               */
+  int32_t precision;          /* gtls_precision                                 */
+  int32_t pass;               /* gtls_pass                                      */
+  int32_t n;                  /* samples                                        */
+  const double* t;            /* [n] times, days, finite and > 0                */
+  const double* y;            /* [n] flux                                       */
+  const double* dy;           /* [n] flux uncertainty, > 0                      */
+  int64_t n_periods;
+  const double* periods;      /* [n_periods] days, > 0                          */
+  int32_t n_durations;        /* D, <= GTLS_MAX_DURATIONS                       */
+  int32_t max_width;          /* maxDuration (core.py:608-612): max width, made even */
+  const int32_t* widths;      /* [D] ascending, >= 1, <= max_width              */
+  const double* overshoot;    /* [D]                                            */
+  const double* templates;    /* [D * max_width] row d: 1 - template (core.py:753-754) */
+  double depth_min;           /* transit_depth_min                              */
+  int32_t skip_point;         /* int(1/T0_fit_margin) or 0x7f800000             */
+  int32_t batch;              /* periods per duration-union batch, >= 1         */
+  float span;                 /* max(t) - min(t) as float                       */
+  int32_t reserved;
+  double* chi2_out;           /* [n_periods]                                    */
+  int64_t* loc_out;           /* [n_periods] or NULL                            */
+  gtls_timing* timing;        /* host, or NULL                                  */
+} gtls_search_desc;
+
+#define GTLS_MAX_DURATIONS 1024
+
+int gtls_search(gtls_ctx* ctx, const gtls_search_desc* desc, void* stream);
+
+/*
+ * Spectra of a chi2 array (stats.spectra, stats.py:95-122, with the
+ * running median of helpers.py:91-106).  mask may be NULL (nothing masked);
+ * masked entries are left out of every min/mean/std/max/median as numpy.ma
+ * does.  Outputs sr, power_raw, power: [n]; sde_raw and sde: host scalars.
+ * kernel = oversampling_factor * 30, made odd.  Synchronises the stream.
+ */
+int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t n,
+                 double oversampling_factor, double* sr, double* power_raw, double* power,
+                 double* sde_raw, double* sde, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GTLS_B200_H */

@@ -1,0 +1,151 @@
+"""CUDA search kernels against the oracle and the reference's recorded outputs.
+
+Bars: FP64 chi2 within 1e-9 relative of the FP64 oracle and identical argmin
+(duration, start) locations; FP32 chi2 within 2e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import tls_oracle as O
+from conftest import golden, search_inputs
+
+pytestmark = pytest.mark.gpu
+RTOL64 = 1e-9
+RTOL32 = 2e-6
+
+
+def _curve(s):
+    from gtls_b200.core import CurveOnDevice
+    return CurveOnDevice(s["t"], s["y"], s["dy"], s["lc"], s["ov"])
+
+
+def test_period_grid_within_one_ulp_of_reference(cuda):
+    from gtls_b200 import grid as G
+    g = golden("grid")
+    for i in range(6):
+        rs, ms, span, pmin, pmax, osf, ntr = g["case%d_args" % i]
+        ref = g["case%d_periods" % i]
+        if len(ref) < 100:
+            continue
+        ours = G.period_grid(rs, ms, span, pmin, pmax, int(osf), int(ntr))
+        assert len(ours) == len(ref)
+        np.testing.assert_array_almost_equal_nulp(ours, ref, nulp=1)
+
+
+def test_duration_ranges_equal_oracle(cuda):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=3, n=19728, span=27.4)
+    span = s["t"].max() - s["t"].min()
+    a = _lib.duration_ranges(s["periods"], span, len(s["t"]))
+    b = O.duration_ranges(s["periods"], span, len(s["t"]))
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("use_dy,batch", [(False, 1), (False, 7), (True, 5), (True, 1000)])
+def test_main_pass_fp64_matches_oracle(cuda, use_dy, batch):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=11, n=1100, span=6.0, use_dy=use_dy)
+    cur = _curve(s)
+    P = s["periods"][::3]
+    chi2, loc = cur.search(P, 1e-5, 8, batch, _lib.GTLS_PASS_MAIN, "fp64", want_loc=True)
+    c_ref, l_ref = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                    s["overshoot"], s["maxd"], 1e-5, 8, batch)
+    np.testing.assert_allclose(chi2.cpu().numpy(), c_ref, rtol=RTOL64)
+    np.testing.assert_array_equal(loc.cpu().numpy(), l_ref)
+
+
+@pytest.mark.parametrize("use_dy", [False, True])
+def test_all_starts_pass_fp64_matches_oracle(cuda, use_dy):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=12, n=900, span=5.0, use_dy=use_dy)
+    cur = _curve(s)
+    P = s["periods"][::9]
+    chi2, loc = cur.search(P, 1e-5, 8, 4, _lib.GTLS_PASS_ALL, "fp64", want_loc=True)
+    c_ref, l_ref = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                    s["overshoot"], s["maxd"], 1e-5, 8, 4, noskip=True)
+    np.testing.assert_allclose(chi2.cpu().numpy(), c_ref, rtol=RTOL64)
+    np.testing.assert_array_equal(loc.cpu().numpy(), l_ref)
+
+
+@pytest.mark.parametrize("skip_point", [O.SKIP_NEVER, 10, 3])
+def test_other_skip_points_match_oracle(cuda, skip_point):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=13, n=700, span=4.0)
+    cur = _curve(s)
+    P = s["periods"][::11]
+    chi2, loc = cur.search(P, 1e-5, skip_point, 3, _lib.GTLS_PASS_MAIN, "fp64", want_loc=True)
+    c_ref, l_ref = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                    s["overshoot"], s["maxd"], 1e-5, skip_point, 3)
+    np.testing.assert_allclose(chi2.cpu().numpy(), c_ref, rtol=RTOL64)
+    np.testing.assert_array_equal(loc.cpu().numpy(), l_ref)
+
+
+def test_matches_reference_kernel_fixtures(cuda):
+    """Against the reference's own kernels (recorded R64 outputs), per period with its own durations."""
+    import torch
+    from gtls_b200 import _lib
+    k = golden("kernels")
+    for i in range(3):
+        t, y, dy = k["case%d_t" % i], k["case%d_y" % i], k["case%d_dy" % i]
+        widths = k["case%d_widths" % i]
+        maxd = int(k["case%d_maxd" % i][0])
+        tm = np.ones((len(widths), maxd))
+        tm[:, : k["case%d_templates" % i].shape[1]] = k["case%d_templates" % i]
+        dev = torch.device("cuda")
+        curve = dict(t=torch.from_numpy(t).to(dev), y=torch.from_numpy(y).to(dev), dy=torch.from_numpy(dy).to(dev),
+                     span=float(np.float32(t.max() - t.min())))
+        tables = dict(widths=torch.from_numpy(widths.astype(np.int32)).to(dev),
+                      overshoot=torch.from_numpy(k["case%d_overshoot" % i]).to(dev),
+                      templates=torch.from_numpy(tm).to(dev), max_width=maxd)
+        P = torch.from_numpy(k["case%d_periods" % i]).to(dev)
+        ref = k["case%d_r64" % i]
+        c1, l1 = _lib.search(curve, P, tables, 1e-5, 8, 1, _lib.GTLS_PASS_MAIN, "fp64")
+        c2, l2 = _lib.search(curve, P, tables, 1e-5, 8, 1, _lib.GTLS_PASS_ALL, "fp64")
+        np.testing.assert_allclose(c1.cpu().numpy(), ref[:, 0], rtol=RTOL64)
+        np.testing.assert_array_equal(l1.cpu().numpy(), ref[:, 1].astype(np.int64))
+        np.testing.assert_allclose(c2.cpu().numpy(), ref[:, 2], rtol=RTOL64)
+        np.testing.assert_array_equal(l2.cpu().numpy(), ref[:, 3].astype(np.int64))
+        c3, _ = _lib.search(curve, P, tables, 1e-5, 8, 1, _lib.GTLS_PASS_MAIN, "fp32")
+        np.testing.assert_allclose(c3.cpu().numpy(), ref[:, 0], rtol=RTOL32)
+
+
+def test_fp32_main_pass_close_to_fp64(cuda):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=14, n=19728, span=27.4)
+    cur = _curve(s)
+    P = s["periods"][::5]
+    c64, l64 = cur.search(P, 1e-5, 8, 83, _lib.GTLS_PASS_MAIN, "fp64", want_loc=True)
+    c32, l32 = cur.search(P, 1e-5, 8, 83, _lib.GTLS_PASS_MAIN, "fp32", want_loc=True)
+    c64, c32 = c64.cpu().numpy(), c32.cpu().numpy()
+    np.testing.assert_allclose(c32, c64, rtol=RTOL32)
+    assert np.mean(l64.cpu().numpy() == l32.cpu().numpy()) > 0.98
+
+
+def test_empty_union_gives_nan(cuda):
+    """A batch whose periods admit none of the widths gets NaN (core.py:722-729)."""
+    from gtls_b200 import _lib
+    s = search_inputs(seed=15, n=800, span=5.0)
+    cur = _curve(s)
+    P = np.array([0.6, 0.61, 2.5e4, 2.6e4])   # very long periods: every width above wmax
+    chi2, loc = cur.search(P, 1e-5, 8, 2, _lib.GTLS_PASS_MAIN, "fp64", want_loc=True)
+    wmin, wmax = O.duration_ranges(P, s["t"].max() - s["t"].min(), len(s["t"]))
+    c = chi2.cpu().numpy()
+    if np.all(s["widths"].min() > wmax[2:]):
+        assert np.all(np.isnan(c[2:])) and np.all(loc.cpu().numpy()[2:] == -1)
+    assert np.all(np.isfinite(c[:2]))
+
+
+def test_spectra_matches_reference_stats(cuda):
+    import torch
+    from gtls_b200 import _lib
+    sp = golden("spectra")
+    for i in range(4):
+        n, osf = sp["case%d" % i]
+        chi2 = torch.from_numpy(sp["case%d_chi2" % i]).cuda()
+        m = sp["case%d_mask" % i]
+        mask = torch.from_numpy(m.astype(np.uint8)).cuda() if m.any() else None
+        SR, praw, power, sde_raw, sde = _lib.spectra(chi2, mask, float(osf))
+        np.testing.assert_allclose(SR.cpu().numpy()[~m], sp["case%d_SR" % i][~m], rtol=1e-12)
+        np.testing.assert_allclose(power.cpu().numpy()[~m], sp["case%d_power" % i][~m], rtol=1e-9, atol=1e-9)
+        np.testing.assert_allclose([sde_raw, sde], sp["case%d_sde" % i], rtol=1e-9)

@@ -1,0 +1,95 @@
+"""Host-side logic against the reference's pure-Python modules (golden fixtures)."""
+import numpy as np
+
+from conftest import golden
+from gtls_b200 import grid as G, template, validate as V
+
+
+def test_validate_inputs_matches_reference():
+    v = golden("validate")
+    t1, y1, dy1 = V.validate_inputs(v["t"].copy(), v["y"].copy(), v["dy"].copy())
+    np.testing.assert_array_equal(t1, v["t1"])
+    np.testing.assert_array_equal(y1, v["y1"])
+    np.testing.assert_array_equal(dy1, v["dy1"])
+    t2, y2, dy2 = V.validate_inputs(v["t"].copy(), v["y"].copy(), None)
+    np.testing.assert_array_equal(t2, v["t2"])
+    np.testing.assert_array_equal(dy2, v["dy2"])
+
+
+def test_validate_errors():
+    import pytest
+    with pytest.raises(ValueError):
+        V.validate_inputs(np.array([1.0, 2.0]), np.array([1.0, 1.0]), None)
+    with pytest.raises(ValueError):
+        V.validate_inputs(np.array([1.0, 1.0, 1.0]), np.array([1.0, 1.0, 1.0]), None)
+
+    class A:
+        pass
+    with pytest.raises(ValueError):
+        V.validate_args(A(), {"R_star": -1})
+    with pytest.raises(ValueError):
+        V.validate_args(A(), {"transit_template": "nope"})
+    a, _ = V.validate_args(A(), {"T0_fit_margin": 0.5})
+    assert a.T0_fit_margin == 0.125
+
+
+def test_duration_grid_matches_reference():
+    g = golden("grid")
+    for i in range(6):
+        p = g["case%d_periods" % i]
+        d = G.duration_grid(p, shortest=1 / 19728, log_step=1.1)
+        np.testing.assert_array_equal(np.asarray(d), g["case%d_durations" % i])
+
+
+def test_ofir_coefficients_reproduce_reference_grid_within_one_ulp():
+    g = golden("grid")
+    for i in range(6):
+        rs, ms, span, pmin, pmax, osf, ntr = g["case%d_args" % i]
+        ref = g["case%d_periods" % i]
+        a3, c, npts, _ = G.ofir_coefficients(rs, ms, span, osf, int(ntr))
+        X = np.arange(npts) + 1.0
+        p = 1 / (a3 * X + c) ** 3 / 86400
+        p = p[(p > pmin) & (p <= pmax)]
+        if len(ref) >= 100:
+            np.testing.assert_array_almost_equal_nulp(p, ref, nulp=1)
+
+
+def test_template_cache_matches_reference_get_cache():
+    c = golden("cache")
+    for i in range(2):
+        durations = c["case%d_durations" % i]
+        mw = int(c["case%d_maxw" % i][0])
+        base = template.reference_transit(mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+        np.testing.assert_array_equal(base, c["case%d_base" % i])
+        ov, lc = template.get_cache(durations, mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+        np.testing.assert_array_equal(ov["width_in_samples"], c["case%d_width" % i])
+        np.testing.assert_array_equal(ov["overshoot"], c["case%d_overshoot" % i])
+        np.testing.assert_array_equal(np.concatenate(list(lc)), c["case%d_lc" % i])
+
+
+def test_device_templates_layout():
+    c = golden("cache")
+    durations = c["case0_durations"]
+    mw = int(c["case0_maxw"][0])
+    ov, lc = template.get_cache(durations, mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+    widths, os_, dd, tm, maxd = template.device_templates(lc, ov)
+    assert np.all(np.diff(widths) > 0) and maxd % 2 == 0 and maxd >= widths.max()
+    for d in range(len(widths)):
+        n = len(lc[d])
+        np.testing.assert_array_equal(tm[d, :n], 1 - lc[d])
+        assert np.all(tm[d, n:] == 1.0)   # 1 - zero padding (core.py:753-754)
+
+
+def test_candidate_selection_matches_reference_sort():
+    import torch
+    import tls_oracle as O
+    from gtls_b200.core import _candidates
+    rng = np.random.default_rng(0)
+    for n in (50, 400, 3000):
+        periods = np.sort(rng.uniform(0.5, 20, n))
+        power = rng.normal(0, 1, n)
+        power[rng.integers(0, n, 5)] = power[3]   # ties keep index order
+        idx, _ = O.select_candidates(np.ma.array(periods), np.ma.array(power))
+        ours = _candidates(torch.from_numpy(power), torch.zeros(n, dtype=torch.uint8), torch.from_numpy(periods),
+                           torch)
+        assert list(ours) == list(idx)
