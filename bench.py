@@ -92,19 +92,19 @@ class Clocks:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+                                          "--format=csv,noheader,nounits", "-lms", "100", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(0.2)
             self.proc.terminate()
             self.proc.wait()
-            self.f.close()
 
     def summary(self):
         if self.proc is None or not os.path.exists(self.path):
@@ -339,8 +339,6 @@ def main():
         "result": {"period": float(out[1]), "true_period": truth["period"], "SDE": float(out[7])},
     }
     if rank == 0:
-        with Clocks(device) as _:
-            pass
         line["clocks"] = clk.summary()
         if not args.no_cpu_baseline:
             cb = cpu_reference(t, y, dy, periods, kw, step, batch)

@@ -188,12 +188,17 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     fin = single_period(cur, period, t, y, dy, transit_depth_min)
 
     chi2_h = _d2h(chi2_dev)
+    # core.py:892-895 wraps raw_chi2 in a masked array without copying, so the
+    # re-searched values written into chi2 (core.py:942,973) also land in the
+    # returned raw_chi2; the main-pass values stay available as chi2_main.
+    chi2_main = raw_chi2
+    raw_chi2 = chi2_h.copy()
     mask_h = _d2h(mask_dev).astype(bool)
     power_h = _d2h(power_dev)
     chi2_m = ma.array(chi2_h, mask=mask_h)
     power_m = ma.array(power_h, mask=mask_h)
     periods_m = ma.array(periods, mask=mask_h)
-    diag = dict(batch_periods=S, period_index=best, sde_raw=sde_raw, again=_d2h(again),
+    diag = dict(batch_periods=S, period_index=best, sde_raw=sde_raw, again=_d2h(again), chi2_main=chi2_main,
                 harmonic_indices=h_idx, chi2_harmonics=_d2h(again2), loc=fin["loc"],
                 skip_point=skip, precision=precision)
     return (periods_m, period, fin["raw_duration"], fin["width"], fin["duration"], fin["depth"], fin["T0"],

@@ -45,13 +45,14 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace gtls {
 
 constexpr int kPrepThreads = 1024;
-constexpr int kChiThreads = 256;
+constexpr int kChiThreads = 512;
 constexpr int kR = 9;            // starts per register block (odd: conflict-free strides)
-constexpr int kSplitMinSkip = 64;  // skip >= this: lanes split the block offset rho
+constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset rho
 
 // ---------------------------------------------------------------- precision
 template <typename Real> struct Tr;
@@ -242,10 +243,11 @@ prepare_kernel(const double* __restrict__ t, const double2* __restrict__ vw, int
   const int pl = blockIdx.x;
   const double P = periods[pl];
   const int M = n + maxd;
+  const int Mrec = (M + 1) & ~1;   // record row stride, even
   double* phi = scr_phi + (size_t)pl * n;
   double* key = scr_key + (size_t)pl * n;
   int* idx = scr_idx + (size_t)pl * n;
-  R2* out = rec + (size_t)pl * M;
+  R2* out = rec + (size_t)pl * Mrec;
   Pv* pre = pv + (size_t)pl * (M + 1);
 
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
@@ -330,6 +332,8 @@ __device__ __forceinline__ void best_update(Best& b, double v, long long loc) {
 
 struct Chi2Args {
   int n, maxd, M;
+  int Mrec;                 // record row stride (M rounded up to even)
+  int* status;              // device status word (bit 0: tile copy did not complete)
   int tile;                 // starts per CTA tile
   int ntiles;
   int pass;                 // GTLS_PASS_MAIN / GTLS_PASS_ALL
@@ -348,26 +352,27 @@ struct Chi2Args {
   long long* part_loc;      // [chunk * ntiles]
 };
 
-// Mean depth of the window [k, k+w): -(sum v)/w  (calcAverageFromCumsum, GPUFun.py:366-375)
-__device__ __forceinline__ double window_mean(const double* pre, int k, int w) {
-  return -(pre[k + w] - pre[k]) / (double)w;
+// Mean depth of the window [k, k+w): -(sum v)/w  (calcAverageFromCumsum, GPUFun.py:366-375),
+// with 1/w computed once per duration.
+__device__ __forceinline__ double window_mean(const double* pre, int k, int w, double inv_w) {
+  return -(pre[k + w] - pre[k]) * inv_w;
 }
-__device__ __forceinline__ float window_mean(const float2* pre, int k, int w) {
+__device__ __forceinline__ float window_mean(const float2* pre, int k, int w, float inv_w) {
   float2 a = pre[k + w], b = pre[k];
   // two-diff of the high parts, then the low parts
   float s = a.x - b.x;
   float bb = s - a.x;
   float e = (a.x - (s - bb)) - (b.x + bb);
   e += a.y - b.y;
-  return -(s + e) / (float)w;
+  return -(s + e) * inv_w;
 }
 
 // Value of start k for duration d from its sums (B, C).
 template <typename Real>
-__device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::Pv* pre, int k, int w,
+__device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::Pv* pre, int k, int w, Real inv_w,
                                            Real os, Real B, Real C, double depth_min, double ebase,
                                            double sentinel, long long loc) {
-  Real mean = window_mean(pre, k, w);
+  Real mean = window_mean(pre, k, w, inv_w);
   if ((double)mean > depth_min) {
     Real c = mean * os * (Real)2;
     Real delta = c * ((Real)2 * B + c * C);
@@ -377,35 +382,45 @@ __device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::
   }
 }
 
-// Correlate one template offset rho of R consecutive starts (start blocks
-// jb .. jb+R-1, start k = j*s) with the tile: aB[r] += sum_q T[q*s+rho] u[(jb+r+q)*s+rho].
-// Q template blocks are processed R at a time; template rows are zero beyond w.
+// Correlate template offset rho of kR consecutive starts with the tile:
+//   aB[r] += sum_{q<Q} T[q*s + rho] * u[base + (r+q)*s],  aC[r] likewise with (T^2, w)
+// where base = jb*s + rho - k0 addresses start block jb.  A sliding window of
+// kR records in registers gives one shared-memory load and one template load
+// per kR multiply-add pairs (slot of record q+r is (q+r) % kR; the q loop is
+// unrolled by kR so every slot index is a constant).  Template rows are zero
+// at and beyond w.  Loads past the tile are clamped to its last record: for a
+// start inside the tile they only meet those zero template entries, and the
+// sums of starts past the tile are discarded.
 template <typename Real, bool kTwoLevel>
-__device__ __forceinline__ void correlate_rho(const typename Tr<Real>::R2* __restrict__ tile, int L,
-                                              int base /* jb*s + rho - k0 */, int s,
-                                              const typename Tr<Real>::R2* __restrict__ trow, int rho,
-                                              int Q, Real (&aB)[kR], Real (&aC)[kR]) {
+__device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restrict__ tile, int L, int base, int s,
+                                          const typename Tr<Real>::R2* __restrict__ trow, int rho, int Q,
+                                          Real (&aB)[kR], Real (&aC)[kR]) {
   using R2 = typename Tr<Real>::R2;
+  R2 xs[kR];
+  const int last = L - 1;
+#pragma unroll
+  for (int i = 0; i < kR - 1; ++i) xs[i] = tile[min(base + i * s, last)];
   Real pB[kR], pC[kR];
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    pB[r] = (Real)0;
-    pC[r] = (Real)0;
+    pB[r] = kTwoLevel ? (Real)0 : aB[r];
+    pC[r] = kTwoLevel ? (Real)0 : aC[r];
   }
+  int pos = base + (kR - 1) * s;
+  int toff = rho;
   for (int q0 = 0; q0 < Q; q0 += kR) {
-    R2 x[2 * kR - 1];
-#pragma unroll
-    for (int i = 0; i < 2 * kR - 1; ++i) {
-      int pos = base + (q0 + i) * s;
-      x[i] = pos < L ? tile[pos] : R2{(Real)0, (Real)0};
-    }
 #pragma unroll
     for (int qq = 0; qq < kR; ++qq) {
-      R2 tq = trow[(q0 + qq) * s + rho];
+      if (q0 + qq >= Q) break;
+      xs[(qq + kR - 1) % kR] = tile[min(pos, last)];
+      const R2 tq = trow[toff];
+      pos += s;
+      toff += s;
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
-        pB[r] = fma(tq.x, x[qq + r].x, pB[r]);
-        pC[r] = fma(tq.y, x[qq + r].y, pC[r]);
+        const R2 x = xs[(qq + r) % kR];
+        pB[r] = fma(tq.x, x.x, pB[r]);
+        pC[r] = fma(tq.y, x.y, pC[r]);
       }
     }
   }
@@ -415,14 +430,141 @@ __device__ __forceinline__ void correlate_rho(const typename Tr<Real>::R2* __res
       aB[r] += pB[r];
       aC[r] += pC[r];
     } else {
-      aB[r] = pB[r] + aB[r];
-      aC[r] = pC[r] + aC[r];
+      aB[r] = pB[r];
+      aC[r] = pC[r];
     }
   }
 }
 
+// Same sums for the lanes-split path: the kR template entries of one block of
+// kR template offsets are loaded together first (kR loads in flight), then the
+// 2*kR-1 records they touch stream through once.
+template <typename Real, bool kTwoLevel>
+__device__ __forceinline__ void correlate_pre(const typename Tr<Real>::R2* __restrict__ tile, int L, int base,
+                                              int s, const typename Tr<Real>::R2* __restrict__ trow, int rho,
+                                              int Q, Real (&aB)[kR], Real (&aC)[kR]) {
+  using R2 = typename Tr<Real>::R2;
+  Real pB[kR], pC[kR];
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    pB[r] = kTwoLevel ? (Real)0 : aB[r];
+    pC[r] = kTwoLevel ? (Real)0 : aC[r];
+  }
+  const int last = L - 1;
+  int toff = rho;
+  for (int q0 = 0; q0 < Q; q0 += kR) {
+    R2 tq[kR];
+#pragma unroll
+    for (int qq = 0; qq < kR; ++qq) tq[qq] = trow[toff + qq * s];
+    toff += kR * s;
+    int pos = base + q0 * s;
+#pragma unroll
+    for (int m = 0; m < 2 * kR - 1; ++m) {
+      const R2 x = tile[min(pos, last)];
+      pos += s;
+#pragma unroll
+      for (int qq = 0; qq < kR; ++qq) {
+        const int r = m - qq;
+        if (r >= 0 && r < kR) {
+          pB[r] = fma(tq[qq].x, x.x, pB[r]);
+          pC[r] = fma(tq[qq].y, x.y, pC[r]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    if (kTwoLevel) {
+      aB[r] += pB[r];
+      aC[r] += pC[r];
+    } else {
+      aB[r] = pB[r];
+      aC[r] = pC[r];
+    }
+  }
+}
+
+// Butterfly reduce-scatter of 2*kR = 18 per-lane values over the warp
+// (9 + 5 + 3 + 2 + 1 shuffles): value i ends, summed over all lanes, in lane
+// kLaneOf[i].  Returns this lane's value (meaningful only in those lanes).
+__constant__ int kLaneOf[2 * kR] = {0, 1, 2, 4, 5, 8, 9, 10, 12, 16, 17, 18, 20, 21, 24, 25, 26, 28};
+
 template <typename Real>
-__global__ void __launch_bounds__(kChiThreads)
+__device__ __forceinline__ Real warp_reduce_scatter18(const Real (&aB)[kR], const Real (&aC)[kR]) {
+  const int lane = threadIdx.x & 31;
+  Real v[18];
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    v[r] = aB[r];
+    v[kR + r] = aC[r];
+  }
+  // level xor 16: keep 9 of 18
+  {
+    const bool hi = lane & 16;
+    Real nv[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      Real send = hi ? v[i] : v[9 + i];
+      Real recv = __shfl_xor_sync(0xffffffffu, send, 16);
+      nv[i] = (hi ? v[9 + i] : v[i]) + recv;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = nv[i];
+  }
+  // level xor 8: keep 5 of 9 (v[9] = 0 pad)
+  {
+    const bool hi = lane & 8;
+    v[9] = (Real)0;
+    Real nv[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      Real send = hi ? v[i] : v[5 + i];
+      Real recv = __shfl_xor_sync(0xffffffffu, send, 8);
+      nv[i] = (hi ? v[5 + i] : v[i]) + recv;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i) v[i] = nv[i];
+  }
+  // level xor 4: keep 3 of 5 (v[5] = 0 pad)
+  {
+    const bool hi = lane & 4;
+    v[5] = (Real)0;
+    Real nv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      Real send = hi ? v[i] : v[3 + i];
+      Real recv = __shfl_xor_sync(0xffffffffu, send, 4);
+      nv[i] = (hi ? v[3 + i] : v[i]) + recv;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = nv[i];
+  }
+  // level xor 2: keep 2 of 3 (v[3] = 0 pad)
+  {
+    const bool hi = lane & 2;
+    v[3] = (Real)0;
+    Real nv[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      Real send = hi ? v[i] : v[2 + i];
+      Real recv = __shfl_xor_sync(0xffffffffu, send, 2);
+      nv[i] = (hi ? v[2 + i] : v[i]) + recv;
+    }
+    v[0] = nv[0];
+    v[1] = nv[1];
+  }
+  // level xor 1: keep 1 of 2
+  {
+    const bool hi = lane & 1;
+    Real send = hi ? v[0] : v[1];
+    Real recv = __shfl_xor_sync(0xffffffffu, send, 1);
+    v[0] = (hi ? v[1] : v[0]) + recv;
+  }
+  return v[0];
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kChiThreads, 1)
 chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Real>::Pv* __restrict__ pv,
             const typename Tr<Real>::R2* __restrict__ trows, Chi2Args a) {
   using R2 = typename Tr<Real>::R2;
@@ -433,6 +575,8 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   __shared__ int task_pre[GTLS_MAX_DURATIONS + 1];
   __shared__ int task_next;
   __shared__ Best red[kChiThreads / 32];
+  __shared__ __align__(8) uint64_t tile_bar;
+  __shared__ int tile_ok;
 
   const int tix = blockIdx.x;
   const int pl = blockIdx.y;
@@ -443,15 +587,21 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   const int k0 = tix * a.tile;
   const int k1 = min(a.n, k0 + a.tile);
   const int L = (k1 - k0) + a.maxd - 1;
-  const R2* src = rec + (size_t)pl * a.M + k0;
+  const R2* src = rec + (size_t)pl * a.Mrec + k0;
   const Pv* pre = pv + (size_t)pl * (a.M + 1);
   const double ebase = *a.ebase;
   const double sentinel = (double)a.n;
   const int lane = threadIdx.x & 31;
 
-  // stage the records [k0, k0 + L) in shared memory
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tile[i] = src[i];
-  // task table: union entries in descending width (heaviest first)
+  // stage the records [k0, k0 + L) in shared memory with one bulk (TMA) copy;
+  // the byte count is rounded up to 16 (the record rows are padded for it)
+  const uint32_t tile_bytes = (uint32_t)(((size_t)L * sizeof(R2) + 15) & ~(size_t)15);
+  if (threadIdx.x == 0) {
+    mbar_init(&tile_bar, 1);
+    mbar_arrive_expect_tx(&tile_bar, tile_bytes);
+    bulk_g2s(tile, src, tile_bytes, &tile_bar);
+  }
+  // task table (overlaps the copy): union entries in descending width (heaviest first)
   if (threadIdx.x == 0) {
     int acc = 0;
     for (int u = 0; u < ucnt; ++u) {
@@ -465,6 +615,8 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
     }
     task_pre[ucnt] = acc;
     task_next = 0;
+    tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
+    if (!tile_ok) atomicOr(a.status, 1);
   }
   __syncthreads();
 
@@ -477,7 +629,7 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
         break;
       }
   }
-  const int ntask = task_pre[ucnt];
+  const int ntask = tile_ok ? task_pre[ucnt] : 0;
   while (true) {
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&task_next, 1);
@@ -495,6 +647,7 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
     const int jhi = (k1 + s - 1) / s;
     const R2* trow = trows + a.trow_off[d];
     const Real os = (Real)a.overshoot[d];
+    const Real inv_w = (Real)1 / (Real)w;
     const long long locb = (long long)upos * a.n;
     Real aB[kR], aC[kR];
 #pragma unroll
@@ -506,27 +659,20 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
       // lanes split the offset rho inside a skip block; one task = kR starts
       const int jb = jlo + sub * kR;
       for (int rho = lane; rho < s; rho += 32)
-        correlate_rho<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+        correlate_pre<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+      const Real mine = warp_reduce_scatter18<Real>(aB, aC);
+      // lane kLaneOf[r] holds B_r, lane kLaneOf[kR + r] holds C_r
+      int r = -1;
 #pragma unroll
-      for (int r = 0; r < kR; ++r) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          aB[r] += __shfl_xor_sync(0xffffffffu, aB[r], o);
-          aC[r] += __shfl_xor_sync(0xffffffffu, aC[r], o);
-        }
-      }
-      if (lane < kR) {
-        Real B = aB[0], C = aC[0];
-#pragma unroll
-        for (int r = 1; r < kR; ++r)
-          if (lane == r) {
-            B = aB[r];
-            C = aC[r];
-          }
-        const int j = jb + lane;
+      for (int i = 0; i < kR; ++i)
+        if (lane == kLaneOf[i]) r = i;
+      const int srcl = r >= 0 ? kLaneOf[kR + r] : lane;
+      const Real C = __shfl_sync(0xffffffffu, mine, srcl);
+      if (r >= 0) {
+        const int j = jb + r;
         if (j < jhi) {
           const int k = j * s;
-          eval_start<Real>(best, pre, k, w, os, B, C, a.depth_min, ebase, sentinel, locb + k);
+          eval_start<Real>(best, pre, k, w, inv_w, os, mine, C, a.depth_min, ebase, sentinel, locb + k);
         }
       }
     } else {
@@ -534,13 +680,13 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
       const int jb = jlo + (sub * 32 + lane) * kR;
       if (jb < jhi) {
         for (int rho = 0; rho < s; ++rho)
-          correlate_rho<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+          correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const int j = jb + r;
           if (j < jhi) {
             const int k = j * s;
-            eval_start<Real>(best, pre, k, w, os, aB[r], aC[r], a.depth_min, ebase, sentinel, locb + k);
+            eval_start<Real>(best, pre, k, w, inv_w, os, aB[r], aC[r], a.depth_min, ebase, sentinel, locb + k);
           }
         }
       }
@@ -669,6 +815,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   const int n = d->n;
   const int maxd = d->max_width;
   const int M = n + maxd;
+  const int Mrec = (M + 1) & ~1;
   const int D = d->n_durations;
   const long long np = d->n_periods;
   const int batch = d->batch;
@@ -709,7 +856,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   carve_size<double>(per_period, n);
   carve_size<double>(per_period, n);
   carve_size<int>(per_period, n);
-  carve_size<R2>(per_period, M);
+  carve_size<R2>(per_period, Mrec);
   carve_size<Pv>(per_period, M + 1);
   carve_size<double>(per_period, ntiles);
   carve_size<long long>(per_period, ntiles);
@@ -735,7 +882,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   carve_size<double>(chunk_bytes, (size_t)chunk * n);
   carve_size<double>(chunk_bytes, (size_t)chunk * n);
   carve_size<int>(chunk_bytes, (size_t)chunk * n);
-  carve_size<R2>(chunk_bytes, (size_t)chunk * M);
+  carve_size<R2>(chunk_bytes, (size_t)chunk * Mrec);
   carve_size<Pv>(chunk_bytes, (size_t)chunk * (M + 1));
   carve_size<double>(chunk_bytes, (size_t)chunk * ntiles);
   carve_size<long long>(chunk_bytes, (size_t)chunk * ntiles);
@@ -757,7 +904,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   double* scr_phi = cv.take<double>((size_t)chunk * n);
   double* scr_key = cv.take<double>((size_t)chunk * n);
   int* scr_idx = cv.take<int>((size_t)chunk * n);
-  R2* rec = cv.take<R2>((size_t)chunk * M);
+  R2* rec = cv.take<R2>((size_t)chunk * Mrec);
   Pv* pv = cv.take<Pv>((size_t)chunk * (M + 1));
   double* part_v = cv.take<double>((size_t)chunk * ntiles);
   long long* part_loc = cv.take<long long>((size_t)chunk * ntiles);
@@ -778,6 +925,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
     for (auto& e : ev) GTLS_TRY_CUDA(ctx, cudaEventCreate(&e));
     GTLS_TRY_CUDA(ctx, cudaEventRecord(ev[0], st));
   }
+  GTLS_TRY_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(int), st));
   curve_setup_kernel<<<1, 1024, 0, st>>>(d->y, d->dy, n, vw, ebase);
   duration_range_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(d->periods, np, d->span, n, wmin, wmax);
   union_kernel<<<(unsigned)nbatch, 256, 0, st>>>(wmin, wmax, np, batch, dwid, D, ucnt, ulist);
@@ -794,6 +942,8 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   ca.n = n;
   ca.maxd = maxd;
   ca.M = M;
+  ca.Mrec = Mrec;
+  ca.status = ctx->status;
   ca.tile = (int)tile;
   ca.ntiles = ntiles;
   ca.pass = d->pass;
@@ -866,6 +1016,11 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
     tm->chi2_starts = starts;
     tm->chi2_fma = fma;
   }
+  // device status word: a tile copy that did not complete within its bound
+  int hst = 0;
+  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(&hst, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GTLS_TRY_CUDA(ctx, cudaStreamSynchronize(st));
+  if (hst != 0) return fail(ctx, GTLS_E_DEVICE, "chi2 kernel: shared-memory tile copy timed out");
   return GTLS_OK;
 }
 
