@@ -250,46 +250,96 @@ prepare_kernel(const double* __restrict__ t, const double2* __restrict__ vw, int
   R2* out = rec + (size_t)pl * Mrec;
   Pv* pre = pv + (size_t)pl * (M + 1);
 
+  constexpr int kB = 4;   // elements per thread in flight in each pass
+  const int stride = blockDim.x * kB;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   // (1) fold and histogram of buckets
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double ph = fold_phase(t[i], P);
-    phi[i] = ph;
-    atomicAdd(&hist[phase_bin(ph, nb_log2)], 1);
+  for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
+    double tv[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      tv[u] = i < n ? t[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) {
+        const double ph = fold_phase(tv[u], P);
+        phi[i] = ph;
+        atomicAdd(&hist[phase_bin(ph, nb_log2)], 1);
+      }
+    }
   }
   __syncthreads();
   block_exclusive_scan_smem(hist, nb, wtmp_i);
   // (2) scatter (phase, index) into bucket slots; afterwards hist[b] is the
   //     end of bucket b and hist[b-1] its start.
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double ph = phi[i];
-    int slot = atomicAdd(&hist[phase_bin(ph, nb_log2)], 1);
-    key[slot] = ph;
-    idx[slot] = i;
+  for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
+    double ph[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      ph[u] = i < n ? phi[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) {
+        const int slot = atomicAdd(&hist[phase_bin(ph[u], nb_log2)], 1);
+        key[slot] = ph[u];
+        idx[slot] = i;
+      }
+    }
   }
   __syncthreads();
   // (3) rank inside the bucket by (phase, original index): the order of a
   //     stable sort by phase.  Gather (u, w) into the sorted position and its
   //     wrapped copy (patchData), keep v for the prefix scan in phi[].
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    double kj = key[j];
-    int ij = idx[j];
-    int b = phase_bin(kj, nb_log2);
-    int s = b == 0 ? 0 : hist[b - 1];
-    int e = hist[b];
-    int rank = s;
-    for (int m = s; m < e; ++m) {
-      double km = key[m];
-      rank += (km < kj) || (km == kj && idx[m] < ij);
+  for (int j0 = threadIdx.x; j0 < n; j0 += stride) {
+    double kj[kB];
+    int ij[kB], rank[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int j = j0 + u * blockDim.x;
+      kj[u] = j < n ? key[j] : 0.0;
+      ij[u] = j < n ? idx[j] : 0;
     }
-    double2 r = vw[ij];
-    R2 o;
-    o.x = (Real)(r.x * r.y);
-    o.y = (Real)r.y;
-    out[rank] = o;
-    if (rank < maxd) out[n + rank] = o;
-    phi[rank] = r.x;
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int j = j0 + u * blockDim.x;
+      rank[u] = 0;
+      if (j < n) {
+        const int b = phase_bin(kj[u], nb_log2);
+        const int s = b == 0 ? 0 : hist[b - 1];
+        const int e = hist[b];
+        int r = s;
+        for (int m = s; m < e; ++m) {
+          const double km = key[m];
+          r += (km < kj[u]) || (km == kj[u] && idx[m] < ij[u]);
+        }
+        rank[u] = r;
+      }
+    }
+    double2 g[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int j = j0 + u * blockDim.x;
+      g[u] = j < n ? vw[ij[u]] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int j = j0 + u * blockDim.x;
+      if (j < n) {
+        R2 o;
+        o.x = (Real)(g[u].x * g[u].y);
+        o.y = (Real)g[u].y;
+        out[rank[u]] = o;
+        if (rank[u] < maxd) out[n + rank[u]] = o;
+        phi[rank[u]] = g[u].x;
+      }
+    }
   }
   __syncthreads();
   // (4) prefix of v over the padded sorted order: pre[0] = 0, pre[r+1] = sum_{q<=r} v_q
@@ -346,6 +396,7 @@ struct Chi2Args {
   const double* overshoot;  // [D]
   const int* union_cnt;     // [nbatch]
   const int* union_list;    // [nbatch * D] ascending duration indices
+  const short* cost_order;  // [nbatch * D] positions in union_list, longest task first
   double depth_min;
   const double* ebase;      // device scalar
   double* part_v;           // [chunk * ntiles]
@@ -408,14 +459,16 @@ __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restric
   }
   int pos = base + (kR - 1) * s;
   int toff = rho;
+  R2 tnext = trow[toff];
   for (int q0 = 0; q0 < Q; q0 += kR) {
 #pragma unroll
     for (int qq = 0; qq < kR; ++qq) {
       if (q0 + qq >= Q) break;
       xs[(qq + kR - 1) % kR] = tile[min(pos, last)];
-      const R2 tq = trow[toff];
+      const R2 tq = tnext;
       pos += s;
       toff += s;
+      tnext = trow[toff];   // next template entry (rows carry one zero block past Q)
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
         const R2 x = xs[(qq + r) % kR];
@@ -573,6 +626,7 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* tile = reinterpret_cast<R2*>(smem_raw);
   __shared__ int task_pre[GTLS_MAX_DURATIONS + 1];
+  __shared__ short task_dur[GTLS_MAX_DURATIONS];
   __shared__ int task_next;
   __shared__ Best red[kChiThreads / 32];
   __shared__ __align__(8) uint64_t tile_bar;
@@ -601,22 +655,37 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
     mbar_arrive_expect_tx(&tile_bar, tile_bytes);
     bulk_g2s(tile, src, tile_bytes, &tile_bar);
   }
-  // task table (overlaps the copy): union entries in descending width (heaviest first)
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int u = 0; u < ucnt; ++u) {
-      int d = ulist[ucnt - 1 - u];
-      int s = a.skips[d];
-      int jlo = (k0 + s - 1) / s, jhi = (k1 + s - 1) / s;
-      int nj = max(0, jhi - jlo);
-      int nt = (s >= kSplitMinSkip) ? (nj + kR - 1) / kR : (nj + 32 * kR - 1) / (32 * kR);
-      task_pre[u] = acc;
-      acc += nt;
+  // task table (warp 0, overlapping the copy): the batch's durations in the
+  // precomputed cost order (longest task first, so the CTA's last tasks are short)
+  const short* corder = a.cost_order + (size_t)bidx * a.D;
+  if (threadIdx.x < 32) {
+    int carry = 0;
+    for (int u0 = 0; u0 < ucnt; u0 += 32) {
+      const int u = u0 + lane;
+      int nt = 0;
+      if (u < ucnt) {
+        task_dur[u] = corder[u];
+        const int d = ulist[corder[u]];
+        const int sk = a.skips[d];
+        const int jlo = (k0 + sk - 1) / sk, jhi = (k1 + sk - 1) / sk;
+        const int nj = max(0, jhi - jlo);
+        nt = (sk >= kSplitMinSkip) ? (nj + kR - 1) / kR : (nj + 32 * kR - 1) / (32 * kR);
+      }
+      int inc = nt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int yv = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += yv;
+      }
+      if (u < ucnt) task_pre[u] = carry + inc - nt;
+      carry += __shfl_sync(0xffffffffu, inc, 31);
     }
-    task_pre[ucnt] = acc;
-    task_next = 0;
-    tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
-    if (!tile_ok) atomicOr(a.status, 1);
+    if (lane == 0) {
+      task_pre[ucnt] = carry;
+      task_next = 0;
+      tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
+      if (!tile_ok) atomicOr(a.status, 1);
+    }
   }
   __syncthreads();
 
@@ -635,10 +704,16 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
     if (lane == 0) tk = atomicAdd(&task_next, 1);
     tk = __shfl_sync(0xffffffffu, tk, 0);
     if (tk >= ntask) break;
-    int u = 0;
-    while (task_pre[u + 1] <= tk) ++u;
+    // binary search: the entry u with task_pre[u] <= tk < task_pre[u + 1]
+    int lo = 0, hi = ucnt - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (task_pre[mid] <= tk) lo = mid;
+      else hi = mid - 1;
+    }
+    const int u = lo;
     const int sub = tk - task_pre[u];
-    const int upos = ucnt - 1 - u;       // position in ascending union order
+    const int upos = task_dur[u];        // position in ascending union order
     const int d = ulist[upos];
     const int w = a.widths[d];
     const int s = a.skips[d];
@@ -754,12 +829,16 @@ __global__ void duration_range_kernel(const double* __restrict__ periods, long l
 }
 
 // One CTA per batch: the ascending list of durations valid for at least one
-// period of the batch (durationBool GPUFun.py:91-105 OR-ed as core.py:704-716).
+// period of the batch (durationBool GPUFun.py:91-105 OR-ed as core.py:704-716),
+// and the same entries ordered by the cost of one chi2 task, longest first
+// (cost_order holds positions in the ascending list).
 __global__ void union_kernel(const int* __restrict__ wmin, const int* __restrict__ wmax, long long np,
-                             int batch, const int* __restrict__ widths, int D, int* __restrict__ union_cnt,
-                             int* __restrict__ union_list) {
+                             int batch, const int* __restrict__ widths, const int* __restrict__ skips, int D,
+                             int* __restrict__ union_cnt, int* __restrict__ union_list,
+                             short* __restrict__ cost_order) {
   __shared__ int flags[GTLS_MAX_DURATIONS];
-  __shared__ int warp_tmp[32];
+  __shared__ int cost[GTLS_MAX_DURATIONS];
+  __shared__ short pos[GTLS_MAX_DURATIONS];
   const long long b = blockIdx.x;
   const long long p0 = b * batch;
   const long long p1 = min(np, p0 + batch);
@@ -770,14 +849,34 @@ __global__ void union_kernel(const int* __restrict__ wmin, const int* __restrict
     flags[d] = any;
   }
   __syncthreads();
-  // ascending compaction
   if (threadIdx.x == 0) {
     int c = 0;
     for (int d = 0; d < D; ++d)
-      if (flags[d]) union_list[b * D + c++] = d;
+      if (flags[d]) {
+        union_list[b * D + c] = d;
+        const int sk = skips[d];
+        const int Qb = ((widths[d] + sk - 1) / sk + kR - 1) / kR;
+        // per-lane work of one task: every rho (thread-group path) or rho / 32 (split path)
+        cost[c] = (sk >= kSplitMinSkip ? (sk + 31) / 32 * 5 / 4 : sk) * Qb;
+        pos[c] = (short)c;
+        ++c;
+      }
     union_cnt[b] = c;
+    // insertion sort by cost, descending (ties: wider first)
+    for (int i = 1; i < c; ++i) {
+      int cv = cost[i];
+      short pv = pos[i];
+      int j = i - 1;
+      while (j >= 0 && (cost[j] < cv || (cost[j] == cv && pos[j] < pv))) {
+        cost[j + 1] = cost[j];
+        pos[j + 1] = pos[j];
+        --j;
+      }
+      cost[j + 1] = cv;
+      pos[j + 1] = pv;
+    }
+    for (int i = 0; i < c; ++i) cost_order[b * D + i] = pos[i];
   }
-  (void)warp_tmp;
 }
 
 // Template rows in the layout the chi2 kernel reads: row d holds (s_i, s_i^2)
@@ -836,12 +935,12 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
     int Qr = (Q + kR - 1) / kR * kR;
     hskip[i] = s;
     hoff[i] = (int)rows_total;
-    hlen[i] = Qr * s;
+    hlen[i] = (Qr + 1) * s;   // one extra zero block: the one-step template prefetch reads it
     rows_total += (size_t)hlen[i];
   }
 
   // tile size: as many starts as fit next to the maxd halo in shared memory
-  const size_t smem_budget = (size_t)ctx->smem_optin - 8 * 1024;
+  const size_t smem_budget = (size_t)ctx->smem_optin - 12 * 1024;   // static shared memory ~10.5 KB
   long long tile = ((long long)(smem_budget / sizeof(R2)) - maxd) / 256 * 256;
   if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
   tile = std::min<long long>(tile, 8192);
@@ -872,6 +971,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   carve_size<int>(fixed, np);
   carve_size<int>(fixed, nbatch);
   carve_size<int>(fixed, nbatch * D);
+  carve_size<short>(fixed, nbatch * D);
   carve_size<int>(fixed, D);
   carve_size<int>(fixed, D);
   carve_size<int>(fixed, D);
@@ -896,6 +996,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   int* wmax = cv.take<int>(np);
   int* ucnt = cv.take<int>(nbatch);
   int* ulist = cv.take<int>(nbatch * D);
+  short* corder = cv.take<short>(nbatch * D);
   int* dskip = cv.take<int>(D);
   int* doff = cv.take<int>(D);
   int* dlen = cv.take<int>(D);
@@ -928,7 +1029,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   GTLS_TRY_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(int), st));
   curve_setup_kernel<<<1, 1024, 0, st>>>(d->y, d->dy, n, vw, ebase);
   duration_range_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(d->periods, np, d->span, n, wmin, wmax);
-  union_kernel<<<(unsigned)nbatch, 256, 0, st>>>(wmin, wmax, np, batch, dwid, D, ucnt, ulist);
+  union_kernel<<<(unsigned)nbatch, 256, 0, st>>>(wmin, wmax, np, batch, dwid, dskip, D, ucnt, ulist, corder);
   template_rows_kernel<Real><<<D, 256, 0, st>>>(d->templates, maxd, dwid, doff, dlen, D, trows);
   ctx->launches += 4;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
@@ -955,6 +1056,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   ca.overshoot = d->overshoot;
   ca.union_cnt = ucnt;
   ca.union_list = ulist;
+  ca.cost_order = corder;
   ca.depth_min = d->depth_min;
   ca.ebase = ebase;
   ca.part_v = part_v;
