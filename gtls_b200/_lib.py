@@ -102,6 +102,10 @@ EXPORTS = {
     "gtls_spectra": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
+    "gtls_spectra_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p,
+                              ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
+    "gtls_noalloc_last_error": ([], ctypes.c_char_p),
 }
 
 

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "spectra.cuh"
 
 namespace gtls {
 
@@ -73,13 +74,8 @@ __global__ void period_reverse_kernel(const double* __restrict__ tmp, const int*
 }
 
 // ---------------------------------------------------------------- spectra
-// stats.spectra (stats.py:95-122) with numpy.ma semantics for masked entries.
-struct SpecState {
-  double mean_sr, std_sr, sde_raw, scale_raw;
-  double sde;
-  int count;
-  int has_median;
-};
+// stats.spectra (stats.py:95-122) with numpy.ma semantics for masked entries
+// (SpecState and the kernel declarations are in spectra.cuh).
 
 __device__ __forceinline__ bool unmasked(const uint8_t* mask, long long i) { return !mask || !mask[i]; }
 

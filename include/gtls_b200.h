@@ -155,6 +155,34 @@ int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t
                  double oversampling_factor, double* sr, double* power_raw, double* power,
                  double* sde_raw, double* sde, void* stream);
 
+/*
+ * Allocation-free spectra (no counterpart in the reference: the reference
+ * always allocates through cupy's memory pool).
+ *
+ * For callers that cannot call cudaMalloc when they compute the SDE: code
+ * running under a fixed memory budget owned by another framework, real-time
+ * loops that forbid allocator calls after start-up, or callers without a
+ * gtls context (creating one allocates).  Same inputs, outputs and results as
+ * gtls_spectra; runs on the current device, needs no context, and calls no
+ * allocator: its scratch is a static device array of
+ * GTLS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit.  Limits and rules:
+ *   - n <= GTLS_NOALLOC_MAX_PERIODS, else GTLS_E_RANGE (nothing launched);
+ *   - all calls on a device share the scratch array, so calls that overlap
+ *     on the GPU race; each call writes every scratch value it reads;
+ *   - the first call on a device looks up the array's address (and loads the
+ *     library's device code there): make it before any stream capture;
+ *   - synchronises the stream; errors are described by
+ *     gtls_noalloc_last_error() (thread-local).
+ */
+#define GTLS_NOALLOC_MAX_PERIODS (1 << 20)
+#define GTLS_NOALLOC_SCRATCH_BYTES ((size_t)8 * 1024 * 1024 + 256)
+
+int gtls_spectra_noalloc(const double* chi2, const uint8_t* mask, int64_t n, double oversampling_factor,
+                         double* sr, double* power_raw, double* power, double* sde_raw, double* sde,
+                         void* stream);
+const char* gtls_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
