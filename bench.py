@@ -43,7 +43,24 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-periods", type=int, default=0,
+                    help="profiling only: keep this many periods spread over the grid (a smaller case of the "
+                         "same kernels); the line then describes that case")
     return ap.parse_args()
+
+
+def traffic_per_period(precision, workload):
+    """DRAM bytes per period of the chi2 kernel from a recorded ncu capture
+    (profiles/chi2_kernel_traffic.txt: lines 'workload precision bytes_per_period'), or None."""
+    path = os.path.join(ROOT, "profiles", "chi2_kernel_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == workload and parts[1] == precision:
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
 
 
 def durations_step_for(periods, n, want):
@@ -229,6 +246,9 @@ def main():
     periods = np.sort(G.period_grid(1.0, 1.0, t.max() - t.min(), kw["period_min"], kw["period_max"],
                                     kw["oversampling_factor"], 2, device=device, ascending=True))
     step = durations_step_for(periods, len(t), n_dur) if n_dur else 1.1
+    if args.max_periods:
+        periods = periods[np.linspace(0, len(periods) - 1, args.max_periods).astype(int)]
+        desc += " [profiling subset: %d periods]" % len(periods)
     durations = G.duration_grid(periods, shortest=1 / len(t), log_step=step)
     mw = int(np.max(durations) * len(y))
     mw += mw % 2
@@ -280,6 +300,9 @@ def main():
     api_kw = dict(period_min=kw["period_min"], period_max=kw["period_max"], batch_periods=batch,
                   duration_grid_step=step, oversampling_factor=kw["oversampling_factor"], precision=args.precision,
                   GPUDeviceID=device)
+    if args.max_periods:
+        api_kw = dict(periods=periods, batch_periods=batch, duration_grid_step=step,
+                      oversampling_factor=kw["oversampling_factor"], precision=args.precision, GPUDeviceID=device)
     model.power(**api_kw)
     torch.cuda.synchronize()
     core.TRANSFER.update(h2d=0, d2h=0)
@@ -315,6 +338,8 @@ def main():
     pipe_tflops = flops / (chi2_ms * 1e-3) / 1e12
     pipe_peak = 148 * (64 if args.precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
 
+    tpp = traffic_per_period(args.precision, args.workload)
+    chunk_periods = len(periods) / max(chunks, 1)
     line = {
         "metric": METRIC, "value": value, "unit": "light curves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -327,10 +352,13 @@ def main():
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step},
         "gpu_launches": int(launches // args.steps),
         "roofline": {"bound": "hbm", "kernel": "chi2_kernel", "achieved": achieved_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+                     "traffic": (tpp * chunk_periods if tpp else None),
+                     "traffic_unit": "bytes per launch (ncu dram read+write per period x periods per launch)",
                      "peak_source": peak_src, "launches_per_step": chunks,
                      "avg_launch_ms": chi2_ms / max(chunks, 1),
-                     "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64"},
+                     "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64",
+                     "algorithmic_bytes_per_launch": bytes_per_period * chunk_periods},
         "pipe": {"unit": "TFLOP/s", "fp_pipe": "fp64" if args.precision == "fp64" else "fp32",
                  "achieved": pipe_tflops, "nominal_peak": pipe_peak, "frac": pipe_tflops / pipe_peak,
                  "flops": "2 per (start, template sample) for B and for C"},
