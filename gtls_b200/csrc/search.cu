@@ -227,31 +227,41 @@ __device__ __forceinline__ int phase_bin(double ph, int nb_log2) {
   return b >= nb ? nb - 1 : b;
 }
 
+// Strict order of two slots of the same bucket: by phase, then by original
+// index (the order of a stable argsort).  The 32-bit keys are the in-bucket
+// fractions rounded to float, which preserves every strict inequality; equal
+// keys are decided on the exact FP64 phases, recomputed.
+__device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __restrict__ t, double P) {
+  const float fa = __uint_as_float(a.x), fb = __uint_as_float(b.x);
+  if (fa != fb) return fa < fb;
+  const double pa = fold_phase(t[a.y], P), pb = fold_phase(t[b.y], P);
+  if (pa != pb) return pa < pb;
+  return a.y < b.y;
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kPrepThreads)
 prepare_kernel(const double* __restrict__ t, const double2* __restrict__ vw, int n, int maxd,
-               const double* __restrict__ periods, int nb_log2, double* __restrict__ scr_phi,
-               double* __restrict__ scr_key, int* __restrict__ scr_idx,
-               typename Tr<Real>::R2* __restrict__ rec, typename Tr<Real>::Pv* __restrict__ pv) {
+               const double* __restrict__ periods, int nb_log2, uint2* __restrict__ scr_slot,
+               int* __restrict__ scr_ord, typename Tr<Real>::R2* __restrict__ rec,
+               typename Tr<Real>::Pv* __restrict__ pv) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
   extern __shared__ int hist[];
-  __shared__ double wtmp_d[32];
-  __shared__ float2 wtmp_f[32];
   __shared__ int wtmp_i[32];
+  __shared__ Pv wsum[32];
   const int nb = 1 << nb_log2;
   const int pl = blockIdx.x;
   const double P = periods[pl];
   const int M = n + maxd;
   const int Mrec = (M + 1) & ~1;   // record row stride, even
-  double* phi = scr_phi + (size_t)pl * n;
-  double* key = scr_key + (size_t)pl * n;
-  int* idx = scr_idx + (size_t)pl * n;
+  uint2* slot = scr_slot + (size_t)pl * n;
+  int* ord = scr_ord + (size_t)pl * n;
   R2* out = rec + (size_t)pl * Mrec;
   Pv* pre = pv + (size_t)pl * (M + 1);
-
   constexpr int kB = 4;   // elements per thread in flight in each pass
   const int stride = blockDim.x * kB;
+
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   // (1) fold and histogram of buckets
@@ -265,105 +275,135 @@ prepare_kernel(const double* __restrict__ t, const double2* __restrict__ vw, int
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int i = i0 + u * blockDim.x;
-      if (i < n) {
-        const double ph = fold_phase(tv[u], P);
-        phi[i] = ph;
-        atomicAdd(&hist[phase_bin(ph, nb_log2)], 1);
-      }
+      if (i < n) atomicAdd(&hist[phase_bin(fold_phase(tv[u], P), nb_log2)], 1);
     }
   }
   __syncthreads();
   block_exclusive_scan_smem(hist, nb, wtmp_i);
-  // (2) scatter (phase, index) into bucket slots; afterwards hist[b] is the
-  //     end of bucket b and hist[b-1] its start.
+  // (2) scatter (in-bucket key, index) into bucket slots; afterwards hist[b]
+  //     is the end of bucket b and hist[b-1] its start
   for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
-    double ph[kB];
+    double tv[kB];
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int i = i0 + u * blockDim.x;
-      ph[u] = i < n ? phi[i] : 0.0;
+      tv[u] = i < n ? t[i] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int i = i0 + u * blockDim.x;
       if (i < n) {
-        const int slot = atomicAdd(&hist[phase_bin(ph[u], nb_log2)], 1);
-        key[slot] = ph[u];
-        idx[slot] = i;
+        const double ph = fold_phase(tv[u], P);
+        const int b = phase_bin(ph, nb_log2);
+        const int s = atomicAdd(&hist[b], 1);
+        const float f = (float)(ldexp(ph, nb_log2) - (double)b);
+        slot[s] = make_uint2(__float_as_uint(f), (unsigned)i);
       }
     }
   }
   __syncthreads();
-  // (3) rank inside the bucket by (phase, original index): the order of a
-  //     stable sort by phase.  Gather (u, w) into the sorted position and its
-  //     wrapped copy (patchData), keep v for the prefix scan in phi[].
-  for (int j0 = threadIdx.x; j0 < n; j0 += stride) {
-    double kj[kB];
-    int ij[kB], rank[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int j = j0 + u * blockDim.x;
-      kj[u] = j < n ? key[j] : 0.0;
-      ij[u] = j < n ? idx[j] : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int j = j0 + u * blockDim.x;
-      rank[u] = 0;
-      if (j < n) {
-        const int b = phase_bin(kj[u], nb_log2);
-        const int s = b == 0 ? 0 : hist[b - 1];
-        const int e = hist[b];
-        int r = s;
-        for (int m = s; m < e; ++m) {
-          const double km = key[m];
-          r += (km < kj[u]) || (km == kj[u] && idx[m] < ij[u]);
-        }
-        rank[u] = r;
+  // (3) each thread ranks whole buckets: ord[start + rank] = original index
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int s = b == 0 ? 0 : hist[b - 1];
+    const int e = hist[b];
+    if (e - s == 1) {
+      ord[s] = (int)slot[s].y;
+    } else if (e - s > 1) {
+      for (int j = s; j < e; ++j) {
+        const uint2 sj = slot[j];
+        int r = 0;
+        for (int m = s; m < e; ++m)
+          if (m != j) r += slot_less(slot[m], sj, t, P);
+        ord[s + r] = (int)sj.y;
       }
+    }
+  }
+  __syncthreads();
+  // (4) gather (u, w) into the padded sorted order (patchData) and keep v in
+  //     pre[r + 1] for the scan; indices are clamped so that a malformed
+  //     input can never address outside the curve
+  for (int r0 = threadIdx.x; r0 < M; r0 += stride) {
+    int ii[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int r = r0 + u * blockDim.x;
+      ii[u] = r < M ? ord[r < n ? r : r - n] : 0;
+      ii[u] = min(max(ii[u], 0), n - 1);
     }
     double2 g[kB];
 #pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int j = j0 + u * blockDim.x;
-      g[u] = j < n ? vw[ij[u]] : make_double2(0.0, 0.0);
-    }
+    for (int u = 0; u < kB; ++u) g[u] = vw[ii[u]];
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
-      const int j = j0 + u * blockDim.x;
-      if (j < n) {
+      const int r = r0 + u * blockDim.x;
+      if (r < M) {
         R2 o;
         o.x = (Real)(g[u].x * g[u].y);
         o.y = (Real)g[u].y;
-        out[rank[u]] = o;
-        if (rank[u] < maxd) out[n + rank[u]] = o;
-        phi[rank[u]] = g[u].x;
+        out[r] = o;
+        if constexpr (sizeof(Real) == 8) pre[r + 1] = g[u].x;
+        else pre[r + 1] = ff_from_double(g[u].x);
       }
     }
   }
   __syncthreads();
-  // (4) prefix of v over the padded sorted order: pre[0] = 0, pre[r+1] = sum_{q<=r} v_q
-  const int per = (M + blockDim.x - 1) / blockDim.x;
-  const int beg = min(M, (int)threadIdx.x * per);
-  const int end = min(M, beg + per);
+  // (5) prefix of v in place over pre[1..M]: each warp scans a contiguous
+  //     range (coalesced), then adds the sum of the ranges before it
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int per = (M + nwarp - 1) / nwarp;
+  const int beg = 1 + min(M, wid * per);
+  const int end = 1 + min(M, (wid + 1) * per);
   if constexpr (sizeof(Real) == 8) {
-    double local = 0.0;
-    for (int r = beg; r < end; ++r) local += phi[r < n ? r : r - n];
-    double total;
-    double run = block_exclusive_scan_double(local, wtmp_d, &total);
-    if (threadIdx.x == 0) pre[0] = 0.0;
-    for (int r = beg; r < end; ++r) {
-      run += phi[r < n ? r : r - n];
-      pre[r + 1] = run;
+    double acc = 0.0;
+    for (int r = beg + lane; r < end; r += 32) acc += pre[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) wsum[wid] = acc;
+    __syncthreads();
+    double carry = 0.0;
+    for (int w = 0; w < wid; ++w) carry += wsum[w];
+    if (wid == 0 && lane == 0) pre[0] = 0.0;
+    for (int r0 = beg; r0 < end; r0 += 32) {
+      const int r = r0 + lane;
+      double x = r < end ? pre[r] : 0.0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        double yv = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += yv;
+      }
+      if (r < end) pre[r] = carry + x;
+      carry += __shfl_sync(0xffffffffu, x, 31);
     }
   } else {
-    float2 local = make_float2(0.f, 0.f);
-    for (int r = beg; r < end; ++r) local = ff_add(local, ff_from_double(phi[r < n ? r : r - n]));
-    float2 run = block_exclusive_scan_ff(local, wtmp_f);
-    if (threadIdx.x == 0) pre[0] = make_float2(0.f, 0.f);
-    for (int r = beg; r < end; ++r) {
-      run = ff_add(run, ff_from_double(phi[r < n ? r : r - n]));
-      pre[r + 1] = run;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int r = beg + lane; r < end; r += 32) acc = ff_add(acc, pre[r]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      float2 yv;
+      yv.x = __shfl_xor_sync(0xffffffffu, acc.x, o);
+      yv.y = __shfl_xor_sync(0xffffffffu, acc.y, o);
+      acc = ff_add(acc, yv);
+    }
+    if (lane == 0) wsum[wid] = acc;
+    __syncthreads();
+    float2 carry = make_float2(0.f, 0.f);
+    for (int w = 0; w < wid; ++w) carry = ff_add(carry, wsum[w]);
+    if (wid == 0 && lane == 0) pre[0] = make_float2(0.f, 0.f);
+    for (int r0 = beg; r0 < end; r0 += 32) {
+      const int r = r0 + lane;
+      float2 x = r < end ? pre[r] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        float2 yv;
+        yv.x = __shfl_up_sync(0xffffffffu, x.x, o);
+        yv.y = __shfl_up_sync(0xffffffffu, x.y, o);
+        if (lane >= o) x = ff_add(yv, x);
+      }
+      if (r < end) pre[r] = ff_add(carry, x);
+      float2 tot;
+      tot.x = __shfl_sync(0xffffffffu, x.x, 31);
+      tot.y = __shfl_sync(0xffffffffu, x.y, 31);
+      carry = ff_add(carry, tot);
     }
   }
 }
@@ -952,8 +992,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
 
   // period chunk sized to the scratch budget
   size_t per_period = 0;
-  carve_size<double>(per_period, n);
-  carve_size<double>(per_period, n);
+  carve_size<uint2>(per_period, n);
   carve_size<int>(per_period, n);
   carve_size<R2>(per_period, Mrec);
   carve_size<Pv>(per_period, M + 1);
@@ -979,8 +1018,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   carve_size<R2>(fixed, rows_total);
   fixed += 16 * 256;
   size_t chunk_bytes = 0;
-  carve_size<double>(chunk_bytes, (size_t)chunk * n);
-  carve_size<double>(chunk_bytes, (size_t)chunk * n);
+  carve_size<uint2>(chunk_bytes, (size_t)chunk * n);
   carve_size<int>(chunk_bytes, (size_t)chunk * n);
   carve_size<R2>(chunk_bytes, (size_t)chunk * Mrec);
   carve_size<Pv>(chunk_bytes, (size_t)chunk * (M + 1));
@@ -1002,9 +1040,8 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   int* dlen = cv.take<int>(D);
   int* dwid = cv.take<int>(D);
   R2* trows = cv.take<R2>(rows_total);
-  double* scr_phi = cv.take<double>((size_t)chunk * n);
-  double* scr_key = cv.take<double>((size_t)chunk * n);
-  int* scr_idx = cv.take<int>((size_t)chunk * n);
+  uint2* scr_slot = cv.take<uint2>((size_t)chunk * n);
+  int* scr_ord = cv.take<int>((size_t)chunk * n);
   R2* rec = cv.take<R2>((size_t)chunk * Mrec);
   Pv* pv = cv.take<Pv>((size_t)chunk * (M + 1));
   double* part_v = cv.take<double>((size_t)chunk * ntiles);
@@ -1069,7 +1106,7 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
       GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[0], st));
     }
     prepare_kernel<Real><<<cnt, kPrepThreads, smem_prep, st>>>(d->t, vw, n, maxd, d->periods + p0, nb_log2,
-                                                               scr_phi, scr_key, scr_idx, rec, pv);
+                                                               scr_slot, scr_ord, rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
     ca.p_global0 = p0;
     dim3 grid(ntiles, cnt);
