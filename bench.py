@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-periods", type=int, default=0,
                     help="profiling only: keep this many periods spread over the grid (a smaller case of the "
@@ -193,8 +193,58 @@ def cpu_reference(t, y, dy, periods, kw, step, batch_hint, budget_s=15.0, seed=0
                 seconds_per_curve=total)
 
 
+def bench_refine(args):
+    """Adjoint refinement workload: 1,024 curves x 20,000 samples, 6 parameters
+    each; one step = 50 batched Adam iterations (model chi2 forward + adjoint)."""
+    import torch
+    from gtls_b200 import _lib, refine, synthetic
+    curves, truth, start, scales = synthetic.refinement_set(n_curves=1024, n=20000, seed=0)
+    t, y, w, off = refine.pack_curves(curves, "cuda")
+    p0 = torch.from_numpy(start).cuda()
+    sc = torch.from_numpy(scales).cuda()
+    for _ in range(args.warmup):
+        refine.refine(p0, sc, t, y, w, off, steps=50)
+    torch.cuda.synchronize()
+    launches0 = _lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out, chi, better = refine.refine(p0, sc, t, y, w, off, steps=50)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (_lib.launch_count() - launches0) // args.steps
+    # end to end from host arrays
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    t2, y2, w2, off2 = refine.pack_curves(curves, "cuda")
+    o2, c2, b2 = refine.refine(torch.from_numpy(start).cuda(), torch.from_numpy(scales).cuda(), t2, y2, w2, off2,
+                               steps=50)
+    res = o2.cpu().numpy()
+    torch.cuda.synchronize()
+    e2e_ms = 1000 * (time.perf_counter() - a)
+    samples = int(off[-1].item())
+    chi_start = refine.model_chi2_function().apply(p0, t, y, w, off)
+    gain = float(torch.median(chi_start - chi).item())
+    line = {"metric": "light curves/s (adjoint refinement, 50 Adam steps, 1,024 x 20,000 samples)",
+            "value": 1024 * 1000.0 / ms, "unit": "light curves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cfg5: 1,024 curves x 20,000 samples, (P,T0,D,depth,u1,u2), 50 Adam steps",
+                       "samples": samples},
+            "e2e": {"value": 1024 * 1000.0 / e2e_ms, "unit": "light curves/s",
+                    "h2d_bytes_per_step": int(samples * 24 + 1025 * 8 + 2 * 1024 * 48),
+                    "d2h_bytes_per_step": 1024 * 48, "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "result": {"improved_fraction": float(better.float().mean()), "median_chi2_decrease": gain}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "cfg5":
+        return bench_refine(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -106,6 +106,11 @@ EXPORTS = {
                               ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
     "gtls_noalloc_last_error": ([], ctypes.c_char_p),
+    "gtls_model_chi2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "gtls_model_chi2_grad": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                             ctypes.c_int),
 }
 
 
@@ -251,3 +256,27 @@ def spectra(chi2, mask, oversampling_factor, device=0):
                              _ptr(power), ctypes.byref(sde_raw), ctypes.byref(sde), _stream(torch, device))
     _check(rc, ctx, "gtls_spectra")
     return sr, praw, power, sde_raw.value, sde.value
+
+
+def model_chi2(t, y, w, off, params, device=0):
+    """gtls_model_chi2: chi2 per curve (device tensors, float64; off int64)."""
+    torch = _torch()
+    ctx = context(device)
+    n_curves = int(off.numel()) - 1
+    out = torch.empty(n_curves, dtype=torch.float64, device=params.device)
+    rc = load().gtls_model_chi2(ctx, _ptr(t), _ptr(y), _ptr(w), _ptr(off), n_curves, _ptr(params), _ptr(out),
+                                _stream(torch, device))
+    _check(rc, ctx, "gtls_model_chi2")
+    return out
+
+
+def model_chi2_grad(t, y, w, off, params, grad_chi2, device=0):
+    """gtls_model_chi2_grad: d(sum_c g_c chi2_c)/d params, shape (n_curves, 6)."""
+    torch = _torch()
+    ctx = context(device)
+    n_curves = int(off.numel()) - 1
+    out = torch.empty((n_curves, 6), dtype=torch.float64, device=params.device)
+    rc = load().gtls_model_chi2_grad(ctx, _ptr(t), _ptr(y), _ptr(w), _ptr(off), n_curves, _ptr(params),
+                                     _ptr(grad_chi2), _ptr(out), _stream(torch, device))
+    _check(rc, ctx, "gtls_model_chi2_grad")
+    return out

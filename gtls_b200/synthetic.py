@@ -128,3 +128,34 @@ def small_curve(seed=0, n=1500, span=6.0, period=1.7, depth=3e-3, noise=1e-3, ga
     y *= _transit(t, t0, period, depth, 0.08 * period ** (1 / 3) / 3, [0.45, 0.2])
     s = rng.uniform(0.5 * noise, 1.5 * noise, n) if dy else None
     return t, y, s
+
+
+def refinement_set(n_curves=1024, n=20000, seed=0, noise=1e-3, depth_range=(100e-6, 2000e-6)):
+    """Light curves with transits and perturbed starting parameters for the
+    adjoint refinement: n samples at 2-min cadence, P log-U(1, 13) d, depth
+    log-U(100, 2000) ppm, white noise 1e-3 (dy given).  Starting parameters are
+    the truth moved by up to half an Ofir grid step in P, half a cadence in T0,
+    5% in duration and 10% in depth, with the default limb darkening.
+    Returns (curves [(t, y, dy)], truth (n_curves x 6), start (n_curves x 6),
+    scales (6,) per curve)."""
+    rng = np.random.default_rng(20_000 + seed)
+    cad = 2.0 / DAY_MIN
+    curves, truth, start, scales = [], [], [], []
+    for c in range(n_curves):
+        period = float(np.exp(rng.uniform(np.log(1.0), np.log(13.0))))
+        depth = float(np.exp(rng.uniform(np.log(depth_range[0]), np.log(depth_range[1]))))
+        t = 100.0 + np.arange(n) * cad
+        span = t[-1] - t[0]
+        t0 = t[0] + rng.uniform(0.2, 0.8) * period
+        dur = 0.13 * period ** (1.0 / 3.0) / 3.0
+        u = [0.45, 0.2]
+        y = _transit(t, t0, period, depth, dur, u) + rng.normal(0.0, noise, n)
+        dy = np.full(n, noise)
+        # Ofir spacing at this period for a Sun-like star, oversampling 3
+        step_p = period * 2.7e-4 * (period / span) ** (1.0 / 3.0)
+        curves.append((t, y, dy))
+        truth.append([period, t0, dur, depth, u[0], u[1]])
+        start.append([period + rng.uniform(-0.5, 0.5) * step_p, t0 + rng.uniform(-0.5, 0.5) * cad,
+                      dur * (1 + rng.uniform(-0.05, 0.05)), depth * (1 + rng.uniform(-0.1, 0.1)), 0.4804, 0.1867])
+        scales.append([step_p, cad, 0.05 * dur, 0.1 * depth, 0.05, 0.05])
+    return curves, np.array(truth), np.array(start), np.array(scales)

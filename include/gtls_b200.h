@@ -156,6 +156,25 @@ int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t
                  double* sde_raw, double* sde, void* stream);
 
 /*
+ * Chi2 of the unfolded limb-darkened transit model and its gradient, for
+ * n_curves light curves concatenated in t/y/w (curve c owns samples
+ * curve_off[c] .. curve_off[c+1]-1, w = 1/dy^2).  params[6c..6c+5] =
+ * (P, T0, D, depth, u1, u2) of curve c.  No counterpart in the reference
+ * (north-star addition used to refine a search peak below grid resolution).
+ * Model: tau = (t-T0) - P round((t-T0)/P), s = 2 tau / D,
+ * m = 1 - depth B(s) I(s) / I(0), B = sigmoid((1-s^2)/0.05),
+ * I = 1 - u1 (1-mu) - u2 (1-mu)^2, mu = sqrt(max(softplus_200(1-s^2), 1e-300)).
+ * gtls_model_chi2_grad writes grad_params[6c+k] = grad_chi2[c] * dchi2_c/dparam_k,
+ * recomputing the model instead of storing it.
+ */
+int gtls_model_chi2(gtls_ctx* ctx, const double* t, const double* y, const double* w,
+                    const int64_t* curve_off, int32_t n_curves, const double* params,
+                    double* chi2_out, void* stream);
+int gtls_model_chi2_grad(gtls_ctx* ctx, const double* t, const double* y, const double* w,
+                         const int64_t* curve_off, int32_t n_curves, const double* params,
+                         const double* grad_chi2, double* grad_params, void* stream);
+
+/*
  * Allocation-free spectra (no counterpart in the reference: the reference
  * always allocates through cupy's memory pool).
  *
