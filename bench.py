@@ -41,7 +41,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg5"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg4", "cfg5"])
+    ap.add_argument("--curves", type=int, default=32,
+                    help="cfg4: curves per step (every 4096/curves-th curve of the 4,096-curve set)")
+    ap.add_argument("--no-per-curve", action="store_true", help="cfg4: skip the per-curve FP64 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-periods", type=int, default=0,
                     help="profiling only: keep this many periods spread over the grid (a smaller case of the "
@@ -241,10 +244,194 @@ def bench_refine(args):
     return 0
 
 
+CFG4_METRIC = ("light curves/s (batched TLS search of the 4,096-curve synthetic survey set: 5k-70k samples, "
+               "27-1,470 d, per-curve Ofir grids and duration grids)")
+
+
+def cfg4_sample(n_curves):
+    """Every (4096 / n_curves)-th curve of the 4,096-curve set, and the set's
+    total work (sum over curves of samples x trial periods)."""
+    from gtls_b200 import grid as G, synthetic
+    specs = synthetic.batch_cfg4_specs()
+    stride = max(1, 4096 // n_curves)
+    idx = np.arange(0, 4096, stride)[:n_curves]
+    npts = np.array([G.ofir_coefficients(1.0, 1.0, s)[2] for s in specs["span"]])
+    return specs, idx, float(np.sum(specs["n"] * npts))
+
+
+def cpu_reference_work(t, y, dy, budget_s, seed=0):
+    """Seconds of the reference's CPU kernels per (sample x period) of work,
+    measured on one curve of the set (main pass of a random sample of its
+    periods, plus the all-starts re-search share of one search)."""
+    from gtls_b200 import grid as G
+    a3, c, npts, _ = G.ofir_coefficients(1.0, 1.0, t.max() - t.min(), 3, 2)
+    X = np.arange(npts) + 1.0
+    periods = np.sort(1 / (a3 * X + c) ** 3 / 86400)
+    r = cpu_reference(t, y, dy, periods, dict(oversampling_factor=3), 1.1, max(1, len(periods) // 30),
+                      budget_s=budget_s, seed=seed)
+    if r is None:
+        return None, None
+    return r["seconds_per_curve"] / (len(t) * len(periods)), r
+
+
+def bench_batch(args):
+    """cfg4: batched search of a fixed sample of the 4,096-curve set per step."""
+    import types
+    import torch
+    from gtls_b200 import _lib, batch, gtls, synthetic
+    from gtls_b200.validate import validate_args
+    specs, idx, total_work = cfg4_sample(args.curves)
+    curves = [synthetic.light_curve_cfg4(specs, int(i))[:2] for i in idx]
+    desc = ("cfg4: every %d-th of the 4,096 seeded synthetic curves (%d per step); FP32-compensated main pass, "
+            "FP64 re-search of 200 candidates + 5 harmonics per curve" % (4096 // args.curves, len(idx)))
+    if args.impl == "reference":
+        # seconds per unit work of the reference's CPU kernels, measured on the
+        # sample curve of median work, times the sample's work
+        from gtls_b200 import validate as V
+        works = [len(c[0]) for c in curves]
+        steps = []
+        res = None
+        sample_work = None
+        for i in range(args.warmup + args.steps):
+            j = int(np.argsort(works)[len(works) // 2])
+            t, y, dy = V.validate_inputs(curves[j][0], curves[j][1], None)
+            spw, r = cpu_reference_work(t, y, dy, budget_s=3.0 if i < args.warmup else 10.0, seed=i)
+            if spw is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+                return 0
+            if sample_work is None:
+                from gtls_b200 import grid as G
+                sample_work = sum(len(c[0]) * G.ofir_coefficients(1.0, 1.0, np.ptp(c[0]))[2] for c in curves)
+            if i >= args.warmup:
+                steps.append(spw * sample_work)
+                res = r
+        sec = statistics.median(steps)
+        v = len(idx) / sec
+        line = {"metric": CFG4_METRIC, "value": v, "unit": "light curves/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": desc, "curves": len(idx)},
+                "cpu_baseline": dict(value=v, unit="light curves/s", cores=res["cores"], kind="reference",
+                                     sample=res["sample"] + "; per-(sample x period) cost scaled to the step's "
+                                                          "%.3g sample-periods" % sample_work),
+                "e2e": {"value": v, "unit": "light curves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    device = torch.cuda.current_device()
+    opts = types.SimpleNamespace()
+    validate_args(opts, dict(precision=args.precision, use_threads=1, GPUDeviceID=device))
+    prepared = [batch.prepare_curve(t, y, None, opts, device=device) for (t, y) in curves]
+    cs = batch.CurveSetOnDevice(prepared, device=device)
+    work = float(sum(len(p["t"]) * len(p["periods"]) for p in prepared))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cs.dev)
+    for _ in range(args.warmup):
+        batch.search_on_device(cs, opts, keep_spectra=False)
+    torch.cuda.synchronize()
+    launches0 = _lib.launch_count(device)
+    step_ms, timings = [], []
+    with Clocks(device) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            tm = _lib.Timing()
+            e0.record()
+            out = batch.search_on_device(cs, opts, keep_spectra=False, timing=tm)
+            e1.record()
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            timings.append(tm.as_dict())
+    launches = (_lib.launch_count(device) - launches0) // args.steps
+    ms = statistics.mean(step_ms)
+
+    # end to end through the public batched API from host arrays
+    _lib.TRANSFER.update(h2d=0, d2h=0)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    res = batch.gtls_batch(curves).power(precision=args.precision, use_threads=1, GPUDeviceID=device,
+                                         keep_spectra=False)
+    torch.cuda.synchronize()
+    e2e_ms = 1000.0 * (time.perf_counter() - a)
+    h2d, d2h = _lib.TRANSFER["h2d"], _lib.TRANSFER["d2h"]
+
+    chi2_ms = statistics.mean(t["chi2_ms"] for t in timings)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        hbm_peak, peak_src = 6650.0, "fallback"
+    achieved = 24.0 * work / (chi2_ms * 1e-3) / 1e9
+    flops = 2.0 * statistics.mean(t["chi2_fma"] for t in timings)
+    pipe_tflops = flops / (chi2_ms * 1e-3) / 1e12
+    pipe_peak = 148 * (64 if args.precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
+    chunks = timings[0]["chunks"]
+    line = {
+        "metric": CFG4_METRIC, "value": len(idx) * 1000.0 / ms, "unit": "light curves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32" else "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "curves": len(idx), "sample_periods": work,
+                   "work_fraction_of_4096_set": work / total_work,
+                   "full_set_seconds_estimate": ms * 1e-3 * total_work / work,
+                   "l2": "flushed (256 MB write) before every timed step; per-chunk scratch > L2",
+                   "precision": args.precision},
+        "e2e": {"value": len(idx) * 1000.0 / e2e_ms, "unit": "light curves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "chi2_kernel", "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                     "launches_per_step": chunks, "avg_launch_ms": chi2_ms / max(chunks, 1),
+                     "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64"},
+        "pipe": {"unit": "TFLOP/s", "fp_pipe": "fp64" if args.precision == "fp64" else "fp32",
+                 "achieved": pipe_tflops, "nominal_peak": pipe_peak, "frac": pipe_tflops / pipe_peak},
+        "stages_ms": {k: statistics.mean(t[k] for t in timings) for k in
+                      ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
+    }
+    truth = [(specs["period"][i], bool(specs["has_transit"][i])) for i in idx]
+    line["result"] = {"recovered_1pct": int(sum(abs(r.period - p) < 0.01 * p for r, (p, h) in zip(out, truth) if h)),
+                      "with_transit": int(sum(h for _, h in truth))}
+    if not args.no_per_curve:
+        # the plain FP64 per-curve form on the same curves: one gtls().power() each
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        ref64 = [gtls(t, y, verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device)
+                 for (t, y) in curves]
+        torch.cuda.synchronize()
+        pc_ms = 1000.0 * (time.perf_counter() - a)
+        same = [int(np.argmin(np.abs(p["periods"] - r.period))) == o.period_index
+                for p, r, o in zip(prepared, ref64, out)]
+        sde_rel = [abs(o.SDE - r.SDE) / abs(r.SDE) for r, o in zip(ref64, out)]
+        line["per_curve_fp64"] = {"value": len(idx) * 1000.0 / pc_ms, "unit": "light curves/s",
+                                  "ms": pc_ms, "speedup_of_batched_e2e": pc_ms / e2e_ms,
+                                  "best_index_agreement": float(np.mean(same)),
+                                  "sde_max_rel_diff": float(np.max(sde_rel)),
+                                  "note": "gtls(t, y).power(precision='fp64') per curve, host arrays, wall clock"}
+    line["clocks"] = clk.summary()
+    if not args.no_cpu_baseline:
+        from gtls_b200 import validate as V
+        j = int(np.argsort([len(c[0]) for c in curves])[len(curves) // 2])
+        t, y, dy = V.validate_inputs(curves[j][0], curves[j][1], None)
+        spw, r = cpu_reference_work(t, y, dy, budget_s=15.0)
+        if spw is not None:
+            line["cpu_baseline"] = dict(value=len(idx) / (spw * work), unit="light curves/s", cores=r["cores"],
+                                        kind="reference",
+                                        sample=r["sample"] + "; per-(sample x period) cost scaled to the step's "
+                                                             "%.3g sample-periods" % work)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.workload == "cfg5":
         return bench_refine(args)
+    if args.workload == "cfg4":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        return bench_batch(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -87,18 +87,50 @@ class SearchDesc(ctypes.Structure):
     ]
 
 
+class BatchDesc(ctypes.Structure):
+    """Mirror of ``gtls_batch_desc``."""
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("pass_", ctypes.c_int32),
+        ("n_curves", ctypes.c_int32),
+        ("sample_off", ctypes.c_void_p),
+        ("period_off", ctypes.c_void_p),
+        ("dur_off", ctypes.c_void_p),
+        ("tmpl_off", ctypes.c_void_p),
+        ("max_width", ctypes.c_void_p),
+        ("batch", ctypes.c_void_p),
+        ("span", ctypes.c_void_p),
+        ("t", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("dy", ctypes.c_void_p),
+        ("periods", ctypes.c_void_p),
+        ("widths", ctypes.c_void_p),
+        ("overshoot", ctypes.c_void_p),
+        ("templates", ctypes.c_void_p),
+        ("depth_min", ctypes.c_double),
+        ("skip_point", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("chi2_out", ctypes.c_void_p),
+        ("loc_out", ctypes.c_void_p),
+        ("timing", ctypes.c_void_p),
+    ]
+
+
 EXPORTS = {
     "gtls_ctx_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "gtls_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "gtls_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
     "gtls_abi_version": ([], ctypes.c_int),
     "gtls_launch_count": ([ctypes.c_void_p], ctypes.c_int64),
+    "gtls_set_chunk_budget": ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
     "gtls_period_grid": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
                           ctypes.c_double, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p],
                          ctypes.c_int),
     "gtls_duration_ranges": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_int32,
                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "gtls_search": ([ctypes.c_void_p, ctypes.POINTER(SearchDesc), ctypes.c_void_p], ctypes.c_int),
+    "gtls_search_batch": ([ctypes.c_void_p, ctypes.POINTER(BatchDesc), ctypes.c_void_p], ctypes.c_int),
     "gtls_spectra": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
@@ -200,6 +232,12 @@ def launch_count(device=0):
     return int(load().gtls_launch_count(context(device)))
 
 
+def set_chunk_budget(nbytes, device=0):
+    """Per-chunk scratch budget of the searches on ``device`` (bytes)."""
+    ctx = context(device)
+    _check(load().gtls_set_chunk_budget(ctx, int(nbytes)), ctx, "gtls_set_chunk_budget")
+
+
 def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precision, device=0,
            want_loc=True, timing=None):
     """Run gtls_search for one curve.
@@ -239,6 +277,63 @@ def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precisio
     d.timing = ctypes.addressof(timing) if timing is not None else None
     rc = load().gtls_search(ctx, ctypes.byref(d), _stream(torch, device))
     _check(rc, ctx, "gtls_search")
+    return chi2, loc
+
+
+def search_batch(curves, periods, period_off, tables, depth_min, skip_point, batches, pass_, precision,
+                 device=0, want_loc=True, timing=None):
+    """Run gtls_search_batch over many curves.
+
+    ``curves``: dict of concatenated device tensors t, y, dy (float64), host
+    int64 ``sample_off`` [C+1] and host float32 ``span`` [C].
+    ``periods``: concatenated device float64 tensor, ``period_off`` host
+    int64 [C+1].  ``tables``: concatenated device tensors widths (int32),
+    overshoot (float64), templates (float64), host int64 ``dur_off`` [C+1]
+    and ``tmpl_off`` [C], host int32 ``max_width`` [C].  ``batches``: host
+    int32 [C] periods per duration-union batch.  Returns (chi2, loc) device
+    tensors over all curves' periods.
+    """
+    torch = _torch()
+    ctx = context(device)
+    n_curves = len(curves["span"])
+    total = int(period_off[-1])
+    dev = periods.device
+    chi2 = torch.empty(total, dtype=torch.float64, device=dev)
+    loc = torch.empty(total, dtype=torch.int64, device=dev) if want_loc else None
+    host = dict(
+        sample_off=np.ascontiguousarray(curves["sample_off"], dtype=np.int64),
+        period_off=np.ascontiguousarray(period_off, dtype=np.int64),
+        dur_off=np.ascontiguousarray(tables["dur_off"], dtype=np.int64),
+        tmpl_off=np.ascontiguousarray(tables["tmpl_off"], dtype=np.int64),
+        max_width=np.ascontiguousarray(tables["max_width"], dtype=np.int32),
+        batch=np.ascontiguousarray(batches, dtype=np.int32),
+        span=np.ascontiguousarray(curves["span"], dtype=np.float32),
+    )
+    for k, a in host.items():
+        want = n_curves + 1 if k in ("sample_off", "period_off", "dur_off") else n_curves
+        if a.shape != (want,):
+            raise ValueError("%s must hold %d values" % (k, want))
+    d = BatchDesc()
+    d.abi_version = ABI_VERSION
+    d.precision = GTLS_FP32 if precision == "fp32" else GTLS_FP64
+    d.pass_ = pass_
+    d.n_curves = n_curves
+    for k, a in host.items():
+        setattr(d, k, a.ctypes.data)
+    d.t = curves["t"].data_ptr()
+    d.y = curves["y"].data_ptr()
+    d.dy = curves["dy"].data_ptr()
+    d.periods = periods.data_ptr()
+    d.widths = tables["widths"].data_ptr()
+    d.overshoot = tables["overshoot"].data_ptr()
+    d.templates = tables["templates"].data_ptr()
+    d.depth_min = float(depth_min)
+    d.skip_point = int(skip_point)
+    d.chi2_out = chi2.data_ptr()
+    d.loc_out = loc.data_ptr() if loc is not None else None
+    d.timing = ctypes.addressof(timing) if timing is not None else None
+    rc = load().gtls_search_batch(ctx, ctypes.byref(d), _stream(torch, device))
+    _check(rc, ctx, "gtls_search_batch")
     return chi2, loc
 
 

@@ -212,17 +212,26 @@ def single_period(cur, period, t, y, dy, transit_depth_min):
     chi2, loc = cur.search(np.array([period]), transit_depth_min, 1, 1, _lib.GTLS_PASS_ALL, "fp64",
                            want_loc=True)
     loc = int(_d2h(loc)[0])
-    n = cur.n
-    wmin, wmax = _lib.duration_ranges(np.array([period]), cur.curve["span"], n, device=cur.device)
-    sel = (cur.widths <= wmax[0]) & (cur.widths >= wmin[0])
-    w_sel = cur.widths[sel]
-    didx = loc // n
-    width = int(w_sel[didx])
-    raw_duration = float(cur.durations[sel][didx])
-    overshoot = float(cur.overshoot[sel][didx])
+    fin = finish_period(cur.widths, cur.durations, cur.overshoot, cur.maxd, cur.curve["span"], period, loc, t, y,
+                        device=cur.device)
+    fin["chi2"] = float(_d2h(chi2)[0])
+    return fin
+
+
+def finish_period(widths, durations, overshoot, maxd, span, period, loc, t, y, device=0, full_stats=True):
+    """Host part of core.search_single_periods (core.py:1420-1505) for the chi2
+    minimum ``loc`` (= duration position * n + start) of ``period``: width,
+    duration, depth, T0 and, with ``full_stats``, transit times and SNRs."""
     t = np.asarray(t, dtype=np.float64)
     y = np.asarray(y, dtype=np.float64)
-    maxd = cur.maxd
+    n = len(t)
+    wmin, wmax = _lib.duration_ranges(np.array([period]), span, n, device=device)
+    sel = (widths <= wmax[0]) & (widths >= wmin[0])
+    w_sel = widths[sel]
+    didx = loc // n
+    width = int(w_sel[didx])
+    raw_duration = float(durations[sel][didx])
+    ovs = float(overshoot[sel][didx])
     phase = (t % period) / period                       # foldCPU core.py:16-20
     rank = np.argsort(phase)
     best_t = np.array(t[rank])
@@ -230,16 +239,23 @@ def single_period(cur, period, t, y, dy, transit_depth_min):
     best_y = np.concatenate((best_y, best_y[:maxd]))
     k0 = loc % n
     mean = best_y[k0:k0 + width].mean()
-    depth = float((1 - mean) * overshoot)
+    depth = float((1 - mean) * ovs)
+    tx = best_t[k0]
+    T0 = tx - int((tx - min(t)) / period) * period - period
+    dur_days = float(stats.calc_duration_days(t, period, T0, raw_duration))
+    out = dict(raw_duration=raw_duration, width=width, duration=dur_days, depth=depth, loc=loc)
+    if not full_stats:
+        T0 = T0 + dur_days / 2
+        if T0 < min(t):
+            T0 = T0 + period
+        out["T0"] = float(T0)
+        return out
     out_tr = np.concatenate((best_y[0:k0], best_y[k0 + width:]))
     snr_fit = (1 - depth) * (width ** 0.5) / np.std(out_tr)
     csum = np.cumsum(out_tr)
     red = np.std((csum[width:] - csum[:-width]) / width)
-    tx = best_t[k0]
-    T0 = tx - int((tx - min(t)) / period) * period - period
     transit_times = np.array(stats.all_transit_times(T0, t, period))
     snr_fit_pink = (1 - depth) / ((np.std(out_tr) ** 2 / width) + (red ** 2 / len(transit_times))) ** 0.5
-    dur_days = float(stats.calc_duration_days(t, period, T0, raw_duration))
     T0 = T0 + dur_days / 2
     transit_times = transit_times + dur_days / 2
     if T0 < min(t):
@@ -253,6 +269,6 @@ def single_period(cur, period, t, y, dy, transit_depth_min):
     with np.errstate(divide="ignore", invalid="ignore"):
         snr = ((1 - np.mean(f_in)) / np.std(flux_ootr)) * len(f_in) ** 0.5
         snr_pink = np.mean(snr_pink_pt) * (len(transit_times) ** 0.5)
-    return dict(raw_duration=raw_duration, width=width, duration=dur_days, depth=depth, T0=float(T0),
-                transit_times=transit_times, snr=float(snr), snr_pink=float(snr_pink), snr_fit=float(snr_fit),
-                snr_fit_pink=float(snr_fit_pink), loc=loc, chi2=float(_d2h(chi2)[0]))
+    out.update(T0=float(T0), transit_times=transit_times, snr=float(snr), snr_pink=float(snr_pink),
+               snr_fit=float(snr_fit), snr_fit_pink=float(snr_fit_pink))
+    return out

@@ -228,6 +228,13 @@ int gtls_abi_version(void) { return GTLS_ABI_VERSION; }
 
 int64_t gtls_launch_count(const gtls_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int gtls_set_chunk_budget(gtls_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return GTLS_E_INVALID;
+  if (bytes < ((uint64_t)1 << 20)) return fail(ctx, GTLS_E_INVALID, "chunk budget must be >= 1 MiB");
+  ctx->chunk_budget = (size_t)bytes;
+  return GTLS_OK;
+}
+
 const char* gtls_last_error(const gtls_ctx* ctx) {
   return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }

@@ -16,6 +16,7 @@ struct gtls_ctx {
   size_t arena_bytes = 0;
   int* status = nullptr;       // device status word(s) written by kernels
   long long launches = 0;      // kernels launched through this context
+  size_t chunk_budget = (size_t)8 << 30;   // per-chunk scratch of a search, bytes
 };
 
 namespace gtls {

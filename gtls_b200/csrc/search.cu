@@ -79,15 +79,75 @@ __device__ __forceinline__ float2 ff_from_double(double v) {
   return make_float2(hi, (float)(v - (double)hi));
 }
 
+// ------------------------------------------------------------ descriptors
+// Per-light-curve parameters and buffers on the device.  A search covers one
+// or many light curves; every kernel finds its curve through these.
+template <typename Real>
+struct CurveDev {
+  const double* t;              // [n] times
+  const double* y;              // [n] flux
+  const double* dy;             // [n] uncertainties
+  const double* periods;        // [np] this curve's trial periods
+  double* chi2_out;             // [np]
+  int64_t* loc_out;             // [np] or NULL
+  double2* vw;                  // [n] (v, w) per original sample (scratch)
+  double* ebase;                // sum v^2 w (scratch)
+  int* wmin;                    // [np] duration range (scratch)
+  int* wmax;
+  const int* widths;            // [D]
+  const double* overshoot;      // [D]
+  const double* templates;      // [D * max_width]
+  const int* skips;             // [D]
+  const int* trow_off;          // [D] offsets into trows
+  const int* trow_len;          // [D]
+  typename Tr<Real>::R2* trows; // template rows (s, s^2), zero-padded
+  int* union_cnt;               // [nbatch]
+  int* union_list;              // [nbatch * D] ascending duration indices
+  short* cost_order;            // [nbatch * D] positions in union_list, longest task first
+  long long np;
+  int n, maxd, M, Mrec, D, max_width, batch, nbatch;
+  int tile, ntiles, nb_log2;
+  float span;
+};
+
+// A run: consecutive periods of one curve inside a chunk of the period list,
+// with the offsets of their scratch rows.  Chunk items and chi2 CTAs are
+// numbered run after run.
+struct Run {
+  int curve;
+  int item0;          // first item (period) of the run in its chunk
+  int count;          // periods in the run
+  int tile0;          // first chi2 CTA of the run in its chunk
+  long long pidx0;    // index of the run's first period within its curve
+  long long slot_off; // element offsets of the run's first row in each scratch array
+  long long rec_off;
+  long long pv_off;
+  long long part_off;
+};
+
+// Largest i in [lo, hi) with key(i) <= x (keys ascending, key(lo) <= x).
+template <typename F>
+__device__ __forceinline__ int upper_find(int lo, int hi, long long x, F key) {
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (key(mid) <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // ------------------------------------------------------------ curve set-up
 // (v, w) per original sample: v = y - 1 (exact), w = 1/(dy*dy)
 // (calcInverseSquaredPatchedDy GPUFun.py:134-142), and E = sum v^2 w
 // (calculate_base_error GPUFun.py:293-312 summed over the n samples).
-__global__ void __launch_bounds__(1024) curve_setup_kernel(const double* __restrict__ y,
-                                                           const double* __restrict__ dy, int n,
-                                                           double2* __restrict__ vw,
-                                                           double* __restrict__ ebase) {
+template <typename Real>
+__global__ void __launch_bounds__(1024) curve_setup_kernel(const CurveDev<Real>* __restrict__ cds) {
   __shared__ double red[1024];
+  const CurveDev<Real>& C = cds[blockIdx.x];
+  const double* __restrict__ y = C.y;
+  const double* __restrict__ dy = C.dy;
+  double2* __restrict__ vw = C.vw;
+  const int n = C.n;
   double acc = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double v = y[i] - 1.0;
@@ -103,7 +163,7 @@ __global__ void __launch_bounds__(1024) curve_setup_kernel(const double* __restr
     if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *ebase = red[0];
+  if (threadIdx.x == 0) *C.ebase = red[0];
 }
 
 // ------------------------------------------------------------ block scans
@@ -241,24 +301,32 @@ __device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __rest
 
 template <typename Real>
 __global__ void __launch_bounds__(kPrepThreads)
-prepare_kernel(const double* __restrict__ t, const double2* __restrict__ vw, int n, int maxd,
-               const double* __restrict__ periods, int nb_log2, uint2* __restrict__ scr_slot,
-               int* __restrict__ scr_ord, typename Tr<Real>::R2* __restrict__ rec,
+prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
+               uint2* __restrict__ scr_slot, int* __restrict__ scr_ord, typename Tr<Real>::R2* __restrict__ rec,
                typename Tr<Real>::Pv* __restrict__ pv) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
   extern __shared__ int hist[];
   __shared__ int wtmp_i[32];
   __shared__ Pv wsum[32];
+  const int item = blockIdx.x;
+  const int ri = upper_find(0, nruns, item, [&](int i) { return (long long)runs[i].item0; });
+  const Run& R = runs[ri];
+  const CurveDev<Real>& C = cds[R.curve];
+  const int local = item - R.item0;
+  const double* __restrict__ t = C.t;
+  const double2* __restrict__ vw = C.vw;
+  const int n = C.n;
+  const int maxd = C.maxd;
+  const int nb_log2 = C.nb_log2;
   const int nb = 1 << nb_log2;
-  const int pl = blockIdx.x;
-  const double P = periods[pl];
-  const int M = n + maxd;
-  const int Mrec = (M + 1) & ~1;   // record row stride, even
-  uint2* slot = scr_slot + (size_t)pl * n;
-  int* ord = scr_ord + (size_t)pl * n;
-  R2* out = rec + (size_t)pl * Mrec;
-  Pv* pre = pv + (size_t)pl * (M + 1);
+  const double P = C.periods[R.pidx0 + local];
+  const int M = C.M;
+  const int Mrec = C.Mrec;
+  uint2* slot = scr_slot + R.slot_off + (size_t)local * n;
+  int* ord = scr_ord + R.slot_off + (size_t)local * n;
+  R2* out = rec + R.rec_off + (size_t)local * Mrec;
+  Pv* pre = pv + R.pv_off + (size_t)local * (M + 1);
   constexpr int kB = 4;   // elements per thread in flight in each pass
   const int stride = blockDim.x * kB;
 
@@ -421,26 +489,12 @@ __device__ __forceinline__ void best_update(Best& b, double v, long long loc) {
 }
 
 struct Chi2Args {
-  int n, maxd, M;
-  int Mrec;                 // record row stride (M rounded up to even)
-  int* status;              // device status word (bit 0: tile copy did not complete)
-  int tile;                 // starts per CTA tile
-  int ntiles;
   int pass;                 // GTLS_PASS_MAIN / GTLS_PASS_ALL
-  int batch;                // periods per union batch
-  long long p_global0;      // global index of the chunk's first period
-  int D;
-  const int* widths;        // [D]
-  const int* skips;         // [D]  (1 for every d in the all-starts pass)
-  const int* trow_off;      // [D]  offset of duration d's template row (in pairs)
-  const double* overshoot;  // [D]
-  const int* union_cnt;     // [nbatch]
-  const int* union_list;    // [nbatch * D] ascending duration indices
-  const short* cost_order;  // [nbatch * D] positions in union_list, longest task first
+  int nruns;
   double depth_min;
-  const double* ebase;      // device scalar
-  double* part_v;           // [chunk * ntiles]
-  long long* part_loc;      // [chunk * ntiles]
+  int* status;              // device status word (bit 0: tile copy did not complete)
+  double* part_v;           // [chunk tiles]
+  long long* part_loc;      // [chunk tiles]
 };
 
 // Mean depth of the window [k, k+w): -(sum v)/w  (calcAverageFromCumsum, GPUFun.py:366-375),
@@ -658,8 +712,9 @@ __device__ __forceinline__ Real warp_reduce_scatter18(const Real (&aB)[kR], cons
 
 template <typename Real>
 __global__ void __launch_bounds__(kChiThreads, 1)
-chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Real>::Pv* __restrict__ pv,
-            const typename Tr<Real>::R2* __restrict__ trows, Chi2Args a) {
+chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs,
+            const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Real>::Pv* __restrict__ pv,
+            Chi2Args a) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
   constexpr bool kTwoLevel = sizeof(Real) == 4;
@@ -672,19 +727,26 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   __shared__ __align__(8) uint64_t tile_bar;
   __shared__ int tile_ok;
 
-  const int tix = blockIdx.x;
-  const int pl = blockIdx.y;
-  const long long pg = a.p_global0 + pl;
-  const int bidx = (int)(pg / a.batch);
-  const int ucnt = a.union_cnt[bidx];
-  const int* ulist = a.union_list + (size_t)bidx * a.D;
-  const int k0 = tix * a.tile;
-  const int k1 = min(a.n, k0 + a.tile);
-  const int L = (k1 - k0) + a.maxd - 1;
-  const R2* src = rec + (size_t)pl * a.Mrec + k0;
-  const Pv* pre = pv + (size_t)pl * (a.M + 1);
-  const double ebase = *a.ebase;
-  const double sentinel = (double)a.n;
+  const int cta = blockIdx.x;
+  const int ri = upper_find(0, a.nruns, cta, [&](int i) { return (long long)runs[i].tile0; });
+  const Run& R = runs[ri];
+  const CurveDev<Real>& C = cds[R.curve];
+  const int local = (cta - R.tile0) / C.ntiles;
+  const int tix = (cta - R.tile0) - local * C.ntiles;
+  const long long pg = R.pidx0 + local;       // period index within the curve
+  const int bidx = (int)(pg / C.batch);
+  const int D = C.D;
+  const int n = C.n;
+  const int ucnt = C.union_cnt[bidx];
+  const int* ulist = C.union_list + (size_t)bidx * D;
+  const int k0 = tix * C.tile;
+  const int k1 = min(n, k0 + C.tile);
+  const int L = (k1 - k0) + C.maxd - 1;
+  const R2* src = rec + R.rec_off + (size_t)local * C.Mrec + k0;
+  const Pv* pre = pv + R.pv_off + (size_t)local * (C.M + 1);
+  const double ebase = *C.ebase;
+  const double sentinel = (double)n;
+  const int* __restrict__ skips = C.skips;
   const int lane = threadIdx.x & 31;
 
   // stage the records [k0, k0 + L) in shared memory with one bulk (TMA) copy;
@@ -697,7 +759,7 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   }
   // task table (warp 0, overlapping the copy): the batch's durations in the
   // precomputed cost order (longest task first, so the CTA's last tasks are short)
-  const short* corder = a.cost_order + (size_t)bidx * a.D;
+  const short* corder = C.cost_order + (size_t)bidx * D;
   if (threadIdx.x < 32) {
     int carry = 0;
     for (int u0 = 0; u0 < ucnt; u0 += 32) {
@@ -706,7 +768,7 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
       if (u < ucnt) {
         task_dur[u] = corder[u];
         const int d = ulist[corder[u]];
-        const int sk = a.skips[d];
+        const int sk = skips[d];
         const int jlo = (k0 + sk - 1) / sk, jhi = (k1 + sk - 1) / sk;
         const int nj = max(0, jhi - jlo);
         nt = (sk >= kSplitMinSkip) ? (nj + kR - 1) / kR : (nj + 32 * kR - 1) / (32 * kR);
@@ -731,10 +793,10 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
 
   Best best{INFINITY, 0x7fffffffffffffffLL};
   // the first start skipped by k % skip != 0 carries the value n (GPUFun.py:407,409)
-  if (a.pass == GTLS_PASS_MAIN && k0 == 0 && threadIdx.x == 0 && a.n > 1) {
+  if (a.pass == GTLS_PASS_MAIN && k0 == 0 && threadIdx.x == 0 && n > 1) {
     for (int u = 0; u < ucnt; ++u)
-      if (a.skips[ulist[u]] > 1) {
-        best_update(best, sentinel, (long long)u * a.n + 1);
+      if (skips[ulist[u]] > 1) {
+        best_update(best, sentinel, (long long)u * n + 1);
         break;
       }
   }
@@ -755,15 +817,15 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
     const int sub = tk - task_pre[u];
     const int upos = task_dur[u];        // position in ascending union order
     const int d = ulist[upos];
-    const int w = a.widths[d];
-    const int s = a.skips[d];
+    const int w = C.widths[d];
+    const int s = skips[d];
     const int Q = (w + s - 1) / s;
     const int jlo = (k0 + s - 1) / s;
     const int jhi = (k1 + s - 1) / s;
-    const R2* trow = trows + a.trow_off[d];
-    const Real os = (Real)a.overshoot[d];
+    const R2* trow = C.trows + C.trow_off[d];
+    const Real os = (Real)C.overshoot[d];
     const Real inv_w = (Real)1 / (Real)w;
-    const long long locb = (long long)upos * a.n;
+    const long long locb = (long long)upos * n;
     Real aB[kR], aC[kR];
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
@@ -819,40 +881,40 @@ chi2_kernel(const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Rea
   if (threadIdx.x == 0) {
     Best b = red[0];
     for (int i = 1; i < kChiThreads / 32; ++i) best_update(b, red[i].v, red[i].loc);
-    a.part_v[(size_t)pl * a.ntiles + tix] = b.v;
-    a.part_loc[(size_t)pl * a.ntiles + tix] = b.loc;
+    a.part_v[cta] = b.v;
+    a.part_loc[cta] = b.loc;
   }
 }
 
-__global__ void finish_kernel(const double* __restrict__ part_v, const long long* __restrict__ part_loc,
-                              int ntiles, int count, long long p_global0, int batch,
-                              const int* __restrict__ union_cnt, double* __restrict__ chi2,
-                              int64_t* __restrict__ loc) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= count) return;
-  long long pg = p_global0 + p;
+template <typename Real>
+__global__ void finish_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
+                              int count, const double* __restrict__ part_v, const long long* __restrict__ part_loc) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= count) return;
+  const int ri = upper_find(0, nruns, item, [&](int i) { return (long long)runs[i].item0; });
+  const Run& R = runs[ri];
+  const CurveDev<Real>& C = cds[R.curve];
+  const int local = item - R.item0;
+  const long long pg = R.pidx0 + local;
   Best b{INFINITY, 0x7fffffffffffffffLL};
-  if (union_cnt[pg / batch] == 0) {
+  if (C.union_cnt[pg / C.batch] == 0) {
     b.v = NAN;
     b.loc = -1;
   } else {
-    for (int i = 0; i < ntiles; ++i) best_update(b, part_v[(size_t)p * ntiles + i], part_loc[(size_t)p * ntiles + i]);
+    const long long c0 = (long long)R.tile0 + (long long)local * C.ntiles;
+    for (int i = 0; i < C.ntiles; ++i) best_update(b, part_v[c0 + i], part_loc[c0 + i]);
   }
-  chi2[pg] = b.v;
-  if (loc) loc[pg] = b.loc;
+  C.chi2_out[pg] = b.v;
+  if (C.loc_out) C.loc_out[pg] = b.loc;
 }
 
 // ------------------------------------------------- durations, unions, rows
 // durationsGrid (GPUFun.py:47-86) with the same operation order.
-__global__ void duration_range_kernel(const double* __restrict__ periods, long long np, float span, int n,
-                                      int* __restrict__ wmin, int* __restrict__ wmax) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= np) return;
+__device__ __forceinline__ void duration_range(double period_days, float span, int n, int* wmin, int* wmax) {
   const double kSecondsPerDay = 86400;
   const double kRsMin = 695508000 * 0.05, kRsMax = 695508000 * 4.0;
   const double kRjup = 69911000;
   float length = span;
-  double period_days = periods[i];
   double nt = length / period_days;
   double corr = (nt + 1.0) / nt;
   double ps = period_days * kSecondsPerDay;
@@ -864,46 +926,70 @@ __global__ void duration_range_kernel(const double* __restrict__ periods, long l
   double dmax = t14max / ps;
   dmin = dmin > 0.15 ? 0.15 : dmin;
   dmax = dmax > 0.15 ? 0.15 : dmax;
-  wmin[i] = (int)floor(dmin * n);
-  wmax[i] = (int)ceil(dmax * n * corr);
+  *wmin = (int)floor(dmin * n);
+  *wmax = (int)ceil(dmax * n * corr);
 }
 
-// One CTA per batch: the ascending list of durations valid for at least one
-// period of the batch (durationBool GPUFun.py:91-105 OR-ed as core.py:704-716),
-// and the same entries ordered by the cost of one chi2 task, longest first
-// (cost_order holds positions in the ascending list).
-__global__ void union_kernel(const int* __restrict__ wmin, const int* __restrict__ wmax, long long np,
-                             int batch, const int* __restrict__ widths, const int* __restrict__ skips, int D,
-                             int* __restrict__ union_cnt, int* __restrict__ union_list,
-                             short* __restrict__ cost_order) {
+__global__ void duration_range_kernel(const double* __restrict__ periods, long long np, float span, int n,
+                                      int* __restrict__ wmin, int* __restrict__ wmax) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  duration_range(periods[i], span, n, &wmin[i], &wmax[i]);
+}
+
+// Duration ranges of every period of every curve (period offsets p_off).
+template <typename Real>
+__global__ void duration_range_batch_kernel(const CurveDev<Real>* __restrict__ cds,
+                                            const long long* __restrict__ p_off, int n_curves) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= p_off[n_curves]) return;
+  const int c = upper_find(0, n_curves, g, [&](int i) { return p_off[i]; });
+  const CurveDev<Real>& C = cds[c];
+  const long long i = g - p_off[c];
+  duration_range(C.periods[i], C.span, C.n, &C.wmin[i], &C.wmax[i]);
+}
+
+// One CTA per union batch (batch offsets b_off): the ascending list of
+// durations valid for at least one period of the batch (durationBool
+// GPUFun.py:91-105 OR-ed as core.py:704-716), and the same entries ordered by
+// the cost of one chi2 task, longest first (cost_order holds positions in
+// the ascending list).
+template <typename Real>
+__global__ void union_kernel(const CurveDev<Real>* __restrict__ cds, const long long* __restrict__ b_off,
+                             int n_curves) {
   __shared__ int flags[GTLS_MAX_DURATIONS];
   __shared__ int cost[GTLS_MAX_DURATIONS];
   __shared__ short pos[GTLS_MAX_DURATIONS];
-  const long long b = blockIdx.x;
-  const long long p0 = b * batch;
-  const long long p1 = min(np, p0 + batch);
+  const long long gb = blockIdx.x;
+  const int c = upper_find(0, n_curves, gb, [&](int i) { return b_off[i]; });
+  const CurveDev<Real>& C = cds[c];
+  const long long b = gb - b_off[c];
+  const int D = C.D;
+  const long long p0 = b * C.batch;
+  const long long p1 = min(C.np, p0 + C.batch);
   for (int d = threadIdx.x; d < D; d += blockDim.x) {
-    int w = widths[d];
+    int w = C.widths[d];
     int any = 0;
-    for (long long p = p0; p < p1 && !any; ++p) any = (w >= wmin[p]) && (w <= wmax[p]);
+    for (long long p = p0; p < p1 && !any; ++p) any = (w >= C.wmin[p]) && (w <= C.wmax[p]);
     flags[d] = any;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    int c = 0;
+    int cnt = 0;
+    int* ulist = C.union_list + b * D;
     for (int d = 0; d < D; ++d)
       if (flags[d]) {
-        union_list[b * D + c] = d;
-        const int sk = skips[d];
-        const int Qb = ((widths[d] + sk - 1) / sk + kR - 1) / kR;
+        ulist[cnt] = d;
+        const int sk = C.skips[d];
+        const int Qb = ((C.widths[d] + sk - 1) / sk + kR - 1) / kR;
         // per-lane work of one task: every rho (thread-group path) or rho / 32 (split path)
-        cost[c] = (sk >= kSplitMinSkip ? (sk + 31) / 32 * 5 / 4 : sk) * Qb;
-        pos[c] = (short)c;
-        ++c;
+        cost[cnt] = (sk >= kSplitMinSkip ? (sk + 31) / 32 * 5 / 4 : sk) * Qb;
+        pos[cnt] = (short)cnt;
+        ++cnt;
       }
-    union_cnt[b] = c;
+    C.union_cnt[b] = cnt;
     // insertion sort by cost, descending (ties: wider first)
-    for (int i = 1; i < c; ++i) {
+    for (int i = 1; i < cnt; ++i) {
       int cv = cost[i];
       short pv = pos[i];
       int j = i - 1;
@@ -915,27 +1001,27 @@ __global__ void union_kernel(const int* __restrict__ wmin, const int* __restrict
       cost[j + 1] = cv;
       pos[j + 1] = pv;
     }
-    for (int i = 0; i < c; ++i) cost_order[b * D + i] = pos[i];
+    for (int i = 0; i < cnt; ++i) C.cost_order[b * D + i] = pos[i];
   }
 }
 
 // Template rows in the layout the chi2 kernel reads: row d holds (s_i, s_i^2)
-// for i < w_d and zeros up to `len` (a multiple of kR skip blocks).
+// for i < w_d and zeros up to its length.  One CTA per (curve, duration).
 template <typename Real>
-__global__ void template_rows_kernel(const double* __restrict__ templates, int max_width,
-                                     const int* __restrict__ widths, const int* __restrict__ row_off,
-                                     const int* __restrict__ row_len, int D,
-                                     typename Tr<Real>::R2* __restrict__ rows) {
-  const int d = blockIdx.x;
-  if (d >= D) return;
-  const int w = widths[d];
-  const int len = row_len[d];
-  typename Tr<Real>::R2* row = rows + row_off[d];
+__global__ void template_rows_kernel(const CurveDev<Real>* __restrict__ cds, const long long* __restrict__ d_off,
+                                     int n_curves) {
+  const long long gd = blockIdx.x;
+  const int c = upper_find(0, n_curves, gd, [&](int i) { return d_off[i]; });
+  const CurveDev<Real>& C = cds[c];
+  const int d = (int)(gd - d_off[c]);
+  const int w = C.widths[d];
+  const int len = C.trow_len[d];
+  typename Tr<Real>::R2* row = C.trows + C.trow_off[d];
   for (int i = threadIdx.x; i < len; i += blockDim.x) {
-    double s = i < w ? templates[(size_t)d * max_width + i] : 0.0;
+    double sv = i < w ? C.templates[(size_t)d * C.max_width + i] : 0.0;
     typename Tr<Real>::R2 o;
-    o.x = (Real)s;
-    o.y = (Real)(s * s);
+    o.x = (Real)sv;
+    o.y = (Real)(sv * sv);
     row[i] = o;
   }
 }
@@ -947,116 +1033,234 @@ static int nb_log2_for(int n) {
   return k;
 }
 
+// One light curve of a search, as the host sees it.
+struct CurveHost {
+  const double *t, *y, *dy, *periods;
+  double* chi2_out;
+  int64_t* loc_out;
+  const int* widths;
+  const double* overshoot;
+  const double* templates;
+  long long np;
+  int n, D, max_width, batch;
+  float span;
+};
+
 template <typename Real>
-static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st) {
+static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int precision_pass, int skip_point,
+                      double depth_min, gtls_timing* tm, cudaStream_t st) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
-  const int n = d->n;
-  const int maxd = d->max_width;
-  const int M = n + maxd;
-  const int Mrec = (M + 1) & ~1;
-  const int D = d->n_durations;
-  const long long np = d->n_periods;
-  const int batch = d->batch;
-  const long long nbatch = (np + batch - 1) / batch;
-  const bool all = d->pass == GTLS_PASS_ALL;
+  const bool all = precision_pass == GTLS_PASS_ALL;
+  const size_t smem_budget = (size_t)ctx->smem_optin - 12 * 1024;   // static shared memory ~10.5 KB
 
-  // host-side per-duration layout (skip, template row offsets)
-  std::vector<int> hw(D), hskip(D), hoff(D), hlen(D);
-  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(hw.data(), d->widths, sizeof(int) * D, cudaMemcpyDeviceToHost, st));
+  // ---- per-curve layout on the host
+  std::vector<CurveDev<Real>> cd(n_curves);
+  std::vector<std::vector<int>> hw(n_curves), hskip(n_curves), hoff(n_curves), hlen(n_curves);
+  std::vector<long long> p_off(n_curves + 1, 0), b_off(n_curves + 1, 0), d_off(n_curves + 1, 0);
+  size_t fixed = 0, rows_total = 0;
+  for (int c = 0; c < n_curves; ++c) {
+    const CurveHost& h = ch[c];
+    const int D = h.D;
+    hw[c].resize(D);
+    GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(hw[c].data(), h.widths, sizeof(int) * D, cudaMemcpyDeviceToHost, st));
+  }
   GTLS_TRY_CUDA(ctx, cudaStreamSynchronize(st));
-  size_t rows_total = 0;
-  for (int i = 0; i < D; ++i) {
-    int w = hw[i];
-    if (w < 1 || w > maxd || (i > 0 && w <= hw[i - 1]))
-      return fail(ctx, GTLS_E_INVALID, "widths must be ascending, >= 1 and <= max_width");
-    int s = (!all && w > d->skip_point) ? w / d->skip_point : 1;
-    int Q = (w + s - 1) / s;
-    int Qr = (Q + kR - 1) / kR * kR;
-    hskip[i] = s;
-    hoff[i] = (int)rows_total;
-    hlen[i] = (Qr + 1) * s;   // one extra zero block: the one-step template prefetch reads it
-    rows_total += (size_t)hlen[i];
+  for (int c = 0; c < n_curves; ++c) {
+    const CurveHost& h = ch[c];
+    const int n = h.n, D = h.D, maxd = h.max_width;
+    CurveDev<Real>& C = cd[c];
+    std::memset(&C, 0, sizeof(C));
+    hskip[c].resize(D);
+    hoff[c].resize(D);
+    hlen[c].resize(D);
+    int rows = 0;
+    for (int i = 0; i < D; ++i) {
+      const int w = hw[c][i];
+      if (w < 1 || w > maxd || (i > 0 && w <= hw[c][i - 1]))
+        return fail(ctx, GTLS_E_INVALID, "widths must be ascending, >= 1 and <= max_width");
+      const int sk = (!all && w > skip_point) ? w / skip_point : 1;
+      const int Q = (w + sk - 1) / sk;
+      const int Qr = (Q + kR - 1) / kR * kR;
+      hskip[c][i] = sk;
+      hoff[c][i] = rows;
+      hlen[c][i] = (Qr + 1) * sk;   // one extra zero block: the one-step template prefetch reads it
+      rows += hlen[c][i];
+    }
+    long long tile = ((long long)(smem_budget / sizeof(R2)) - maxd) / 256 * 256;
+    if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
+    tile = std::min<long long>(tile, 8192);
+    if (tile > n) tile = (n + 255) / 256 * 256;
+    C.t = h.t;
+    C.y = h.y;
+    C.dy = h.dy;
+    C.periods = h.periods;
+    C.chi2_out = h.chi2_out;
+    C.loc_out = h.loc_out;
+    C.widths = h.widths;
+    C.overshoot = h.overshoot;
+    C.templates = h.templates;
+    C.np = h.np;
+    C.n = n;
+    C.maxd = maxd;
+    C.M = n + maxd;
+    C.Mrec = (C.M + 1) & ~1;
+    C.D = D;
+    C.max_width = maxd;
+    C.batch = h.batch;
+    C.nbatch = (int)((h.np + h.batch - 1) / h.batch);
+    C.tile = (int)tile;
+    C.ntiles = (int)((n + tile - 1) / tile);
+    C.nb_log2 = nb_log2_for(n);
+    C.span = h.span;
+    p_off[c + 1] = p_off[c] + h.np;
+    b_off[c + 1] = b_off[c] + C.nbatch;
+    d_off[c + 1] = d_off[c] + D;
+    carve_size<double2>(fixed, n);
+    carve_size<double>(fixed, 1);
+    carve_size<int>(fixed, h.np);
+    carve_size<int>(fixed, h.np);
+    carve_size<int>(fixed, (size_t)C.nbatch);
+    carve_size<int>(fixed, (size_t)C.nbatch * D);
+    carve_size<short>(fixed, (size_t)C.nbatch * D);
+    carve_size<int>(fixed, 3 * (size_t)D);
+    carve_size<R2>(fixed, (size_t)rows);
+    rows_total += rows;
   }
 
-  // tile size: as many starts as fit next to the maxd halo in shared memory
-  const size_t smem_budget = (size_t)ctx->smem_optin - 12 * 1024;   // static shared memory ~10.5 KB
-  long long tile = ((long long)(smem_budget / sizeof(R2)) - maxd) / 256 * 256;
-  if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
-  tile = std::min<long long>(tile, 8192);
-  if (tile > n) tile = (n + 255) / 256 * 256;
-  const int ntiles = (int)((n + tile - 1) / tile);
-  const size_t smem_chi = (size_t)(tile + maxd) * sizeof(R2);
-  const int nb_log2 = nb_log2_for(n);
-  const size_t smem_prep = sizeof(int) << nb_log2;
+  // ---- chunks of the period list (curve after curve) and their runs
+  const size_t budget = ctx->chunk_budget;
+  std::vector<Run> runs;
+  std::vector<int> chunk_r0, chunk_items, chunk_tiles;
+  std::vector<size_t> chunk_smem_prep, chunk_smem_chi;
+  size_t max_slot = 0, max_rec = 0, max_pv = 0, max_part = 0;
+  {
+    size_t slot = 0, rec = 0, pvs = 0, bytes = 0;
+    int items = 0, tiles = 0;
+    size_t sm_prep = 0, sm_chi = 0;
+    chunk_r0.push_back(0);
+    auto close_chunk = [&]() {
+      if (items == 0) return;
+      chunk_items.push_back(items);
+      chunk_tiles.push_back(tiles);
+      chunk_smem_prep.push_back(sm_prep);
+      chunk_smem_chi.push_back(sm_chi);
+      max_slot = std::max(max_slot, slot);
+      max_rec = std::max(max_rec, rec);
+      max_pv = std::max(max_pv, pvs);
+      max_part = std::max(max_part, (size_t)tiles);
+      chunk_r0.push_back((int)runs.size());
+      slot = rec = pvs = bytes = 0;
+      items = tiles = 0;
+      sm_prep = sm_chi = 0;
+    };
+    for (int c = 0; c < n_curves; ++c) {
+      const CurveDev<Real>& C = cd[c];
+      const size_t per = (size_t)C.n * 12 + (size_t)C.Mrec * sizeof(R2) + (size_t)(C.M + 1) * sizeof(Pv) +
+                         (size_t)C.ntiles * 16;
+      long long p = 0;
+      while (p < C.np) {
+        long long fit = (long long)((budget > bytes ? budget - bytes : 0) / per);
+        fit = std::min<long long>(fit, (long long)INT32_MAX - items);
+        fit = std::min<long long>(fit, ((1LL << 31) - 1 - tiles) / C.ntiles);
+        if (fit <= 0) {
+          if (items == 0) return fail(ctx, GTLS_E_RANGE, "one period does not fit the scratch budget");
+          close_chunk();
+          continue;
+        }
+        const long long take = std::min<long long>(fit, C.np - p);
+        Run r;
+        r.curve = c;
+        r.item0 = items;
+        r.count = (int)take;
+        r.tile0 = tiles;
+        r.pidx0 = p;
+        r.slot_off = (long long)slot;
+        r.rec_off = (long long)rec;
+        r.pv_off = (long long)pvs;
+        r.part_off = tiles;
+        runs.push_back(r);
+        slot += (size_t)take * C.n;
+        rec += (size_t)take * C.Mrec;
+        pvs += (size_t)take * (C.M + 1);
+        bytes += (size_t)take * per;
+        items += (int)take;
+        tiles += (int)(take * C.ntiles);
+        sm_prep = std::max(sm_prep, sizeof(int) << C.nb_log2);
+        sm_chi = std::max(sm_chi, (size_t)(C.tile + C.maxd) * sizeof(R2));
+        p += take;
+      }
+    }
+    close_chunk();
+  }
+  const int nchunks = (int)chunk_items.size();
+  const int nruns_total = (int)runs.size();
 
-  // period chunk sized to the scratch budget
-  size_t per_period = 0;
-  carve_size<uint2>(per_period, n);
-  carve_size<int>(per_period, n);
-  carve_size<R2>(per_period, Mrec);
-  carve_size<Pv>(per_period, M + 1);
-  carve_size<double>(per_period, ntiles);
-  carve_size<long long>(per_period, ntiles);
-  per_period += 6 * 256;
-  const size_t budget = (size_t)8 << 30;
-  long long chunk = std::max<long long>(1, std::min<long long>(np, (long long)(budget / per_period)));
-  chunk = std::min<long long>(chunk, 65535);
-
-  size_t fixed = 0;
-  carve_size<double2>(fixed, n);
-  carve_size<double>(fixed, 1);
-  carve_size<int>(fixed, np);
-  carve_size<int>(fixed, np);
-  carve_size<int>(fixed, nbatch);
-  carve_size<int>(fixed, nbatch * D);
-  carve_size<short>(fixed, nbatch * D);
-  carve_size<int>(fixed, D);
-  carve_size<int>(fixed, D);
-  carve_size<int>(fixed, D);
-  carve_size<int>(fixed, D);
-  carve_size<R2>(fixed, rows_total);
-  fixed += 16 * 256;
-  size_t chunk_bytes = 0;
-  carve_size<uint2>(chunk_bytes, (size_t)chunk * n);
-  carve_size<int>(chunk_bytes, (size_t)chunk * n);
-  carve_size<R2>(chunk_bytes, (size_t)chunk * Mrec);
-  carve_size<Pv>(chunk_bytes, (size_t)chunk * (M + 1));
-  carve_size<double>(chunk_bytes, (size_t)chunk * ntiles);
-  carve_size<long long>(chunk_bytes, (size_t)chunk * ntiles);
-  chunk_bytes += 8 * 256;
-  void* mem = arena(ctx, fixed + chunk_bytes);
+  // ---- arena: fixed per-curve buffers, descriptors, and one chunk of scratch
+  size_t total = fixed;
+  carve_size<CurveDev<Real>>(total, n_curves);
+  carve_size<Run>(total, std::max(1, nruns_total));
+  carve_size<long long>(total, 3 * (size_t)(n_curves + 1));
+  carve_size<uint2>(total, max_slot);
+  carve_size<int>(total, max_slot);
+  carve_size<R2>(total, max_rec);
+  carve_size<Pv>(total, max_pv);
+  carve_size<double>(total, max_part);
+  carve_size<long long>(total, max_part);
+  total += 32 * 256;
+  void* mem = arena(ctx, total);
   if (!mem) return fail(ctx, GTLS_E_NOMEM, "scratch allocation failed");
   Carver cv(mem);
-  double2* vw = cv.take<double2>(n);
-  double* ebase = cv.take<double>(1);
-  int* wmin = cv.take<int>(np);
-  int* wmax = cv.take<int>(np);
-  int* ucnt = cv.take<int>(nbatch);
-  int* ulist = cv.take<int>(nbatch * D);
-  short* corder = cv.take<short>(nbatch * D);
-  int* dskip = cv.take<int>(D);
-  int* doff = cv.take<int>(D);
-  int* dlen = cv.take<int>(D);
-  int* dwid = cv.take<int>(D);
-  R2* trows = cv.take<R2>(rows_total);
-  uint2* scr_slot = cv.take<uint2>((size_t)chunk * n);
-  int* scr_ord = cv.take<int>((size_t)chunk * n);
-  R2* rec = cv.take<R2>((size_t)chunk * Mrec);
-  Pv* pv = cv.take<Pv>((size_t)chunk * (M + 1));
-  double* part_v = cv.take<double>((size_t)chunk * ntiles);
-  long long* part_loc = cv.take<long long>((size_t)chunk * ntiles);
+  for (int c = 0; c < n_curves; ++c) {
+    CurveDev<Real>& C = cd[c];
+    C.vw = cv.take<double2>(C.n);
+    C.ebase = cv.take<double>(1);
+    C.wmin = cv.take<int>(C.np);
+    C.wmax = cv.take<int>(C.np);
+    C.union_cnt = cv.take<int>(C.nbatch);
+    C.union_list = cv.take<int>((size_t)C.nbatch * C.D);
+    C.cost_order = cv.take<short>((size_t)C.nbatch * C.D);
+    int* dint = cv.take<int>(3 * (size_t)C.D);
+    C.skips = dint;
+    C.trow_off = dint + C.D;
+    C.trow_len = dint + 2 * C.D;
+    int rows = 0;
+    for (int i = 0; i < C.D; ++i) rows += hlen[c][i];
+    C.trows = cv.take<R2>(rows);
+    std::vector<int> tmp(3 * (size_t)C.D);
+    std::copy(hskip[c].begin(), hskip[c].end(), tmp.begin());
+    std::copy(hoff[c].begin(), hoff[c].end(), tmp.begin() + C.D);
+    std::copy(hlen[c].begin(), hlen[c].end(), tmp.begin() + 2 * C.D);
+    GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(dint, tmp.data(), sizeof(int) * tmp.size(), cudaMemcpyHostToDevice, st));
+  }
+  CurveDev<Real>* d_cd = cv.take<CurveDev<Real>>(n_curves);
+  Run* d_runs = cv.take<Run>(std::max(1, nruns_total));
+  long long* d_offs = cv.take<long long>(3 * (size_t)(n_curves + 1));
+  uint2* scr_slot = cv.take<uint2>(max_slot);
+  int* scr_ord = cv.take<int>(max_slot);
+  R2* rec = cv.take<R2>(max_rec);
+  Pv* pv = cv.take<Pv>(max_pv);
+  double* part_v = cv.take<double>(max_part);
+  long long* part_loc = cv.take<long long>(max_part);
+  {
+    std::vector<long long> offs(3 * (size_t)(n_curves + 1));
+    std::copy(p_off.begin(), p_off.end(), offs.begin());
+    std::copy(b_off.begin(), b_off.end(), offs.begin() + (n_curves + 1));
+    std::copy(d_off.begin(), d_off.end(), offs.begin() + 2 * (n_curves + 1));
+    GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_cd, cd.data(), sizeof(CurveDev<Real>) * n_curves, cudaMemcpyHostToDevice,
+                                       st));
+    if (nruns_total)
+      GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_runs, runs.data(), sizeof(Run) * nruns_total, cudaMemcpyHostToDevice,
+                                         st));
+    GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_offs, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice,
+                                       st));
+  }
+  const long long* d_poff = d_offs;
+  const long long* d_boff = d_offs + (n_curves + 1);
+  const long long* d_doff = d_offs + 2 * (n_curves + 1);
 
-  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(dskip, hskip.data(), sizeof(int) * D, cudaMemcpyHostToDevice, st));
-  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(doff, hoff.data(), sizeof(int) * D, cudaMemcpyHostToDevice, st));
-  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(dlen, hlen.data(), sizeof(int) * D, cudaMemcpyHostToDevice, st));
-  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(dwid, hw.data(), sizeof(int) * D, cudaMemcpyHostToDevice, st));
-  // the caller's pageable vectors must stay alive until the copies ran
-  GTLS_TRY_CUDA(ctx, cudaStreamSynchronize(st));
-
-  // optional stage timing with CUDA events on the call's stream
-  gtls_timing* tm = d->timing;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // ---- optional stage timing with CUDA events on the call's stream
+  cudaEvent_t ev[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> evc;
   if (tm) {
     std::memset(tm, 0, sizeof(*tm));
@@ -1064,56 +1268,46 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
     GTLS_TRY_CUDA(ctx, cudaEventRecord(ev[0], st));
   }
   GTLS_TRY_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(int), st));
-  curve_setup_kernel<<<1, 1024, 0, st>>>(d->y, d->dy, n, vw, ebase);
-  duration_range_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(d->periods, np, d->span, n, wmin, wmax);
-  union_kernel<<<(unsigned)nbatch, 256, 0, st>>>(wmin, wmax, np, batch, dwid, dskip, D, ucnt, ulist, corder);
-  template_rows_kernel<Real><<<D, 256, 0, st>>>(d->templates, maxd, dwid, doff, dlen, D, trows);
+  curve_setup_kernel<Real><<<n_curves, 1024, 0, st>>>(d_cd);
+  if (p_off[n_curves] > 0)
+    duration_range_batch_kernel<Real><<<(unsigned)((p_off[n_curves] + 255) / 256), 256, 0, st>>>(d_cd, d_poff,
+                                                                                                 n_curves);
+  if (b_off[n_curves] > 0) union_kernel<Real><<<(unsigned)b_off[n_curves], 256, 0, st>>>(d_cd, d_boff, n_curves);
+  template_rows_kernel<Real><<<(unsigned)d_off[n_curves], 256, 0, st>>>(d_cd, d_doff, n_curves);
   ctx->launches += 4;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
   if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(ev[1], st));
 
+  size_t max_prep = 0, max_chi = 0;
+  for (int k = 0; k < nchunks; ++k) {
+    max_prep = std::max(max_prep, chunk_smem_prep[k]);
+    max_chi = std::max(max_chi, chunk_smem_chi[k]);
+  }
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_prep));
+                                          (int)std::max<size_t>(max_prep, 1)));
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_chi));
+                                          (int)std::max<size_t>(max_chi, 1)));
   Chi2Args ca;
-  ca.n = n;
-  ca.maxd = maxd;
-  ca.M = M;
-  ca.Mrec = Mrec;
+  ca.pass = precision_pass;
+  ca.depth_min = depth_min;
   ca.status = ctx->status;
-  ca.tile = (int)tile;
-  ca.ntiles = ntiles;
-  ca.pass = d->pass;
-  ca.batch = batch;
-  ca.D = D;
-  ca.widths = dwid;
-  ca.skips = dskip;
-  ca.trow_off = doff;
-  ca.overshoot = d->overshoot;
-  ca.union_cnt = ucnt;
-  ca.union_list = ulist;
-  ca.cost_order = corder;
-  ca.depth_min = d->depth_min;
-  ca.ebase = ebase;
   ca.part_v = part_v;
   ca.part_loc = part_loc;
-  for (long long p0 = 0; p0 < np; p0 += chunk) {
-    const int cnt = (int)std::min<long long>(chunk, np - p0);
+  for (int k = 0; k < nchunks; ++k) {
+    const int r0 = chunk_r0[k], nr = chunk_r0[k + 1] - r0;
+    const int items = chunk_items[k], tiles = chunk_tiles[k];
     cudaEvent_t e3[4];
     if (tm) {
       for (auto& e : e3) GTLS_TRY_CUDA(ctx, cudaEventCreate(&e));
       GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[0], st));
     }
-    prepare_kernel<Real><<<cnt, kPrepThreads, smem_prep, st>>>(d->t, vw, n, maxd, d->periods + p0, nb_log2,
-                                                               scr_slot, scr_ord, rec, pv);
+    prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, scr_ord,
+                                                                          rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
-    ca.p_global0 = p0;
-    dim3 grid(ntiles, cnt);
-    chi2_kernel<Real><<<grid, kChiThreads, smem_chi, st>>>(rec, pv, trows, ca);
+    ca.nruns = nr;
+    chi2_kernel<Real><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[2], st));
-    finish_kernel<<<(cnt + 127) / 128, 128, 0, st>>>(part_v, part_loc, ntiles, cnt, p0, batch, ucnt, d->chi2_out,
-                                                     d->loc_out);
+    finish_kernel<Real><<<(items + 127) / 128, 128, 0, st>>>(d_cd, d_runs + r0, nr, items, part_v, part_loc);
     if (tm) {
       GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[3], st));
       for (auto& e : e3) evc.push_back(e);
@@ -1137,19 +1331,22 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
     tm->chunks = (int)(evc.size() / 4);
     for (auto e : evc) cudaEventDestroy(e);
     for (auto e : ev) cudaEventDestroy(e);
-    // work counters of the chi2 kernel, from the same layout the kernel uses
-    std::vector<int> hc(nbatch), hl((size_t)nbatch * D);
-    GTLS_TRY_CUDA(ctx, cudaMemcpy(hc.data(), ucnt, sizeof(int) * nbatch, cudaMemcpyDeviceToHost));
-    GTLS_TRY_CUDA(ctx, cudaMemcpy(hl.data(), ulist, sizeof(int) * nbatch * D, cudaMemcpyDeviceToHost));
+    // work counters of the chi2 kernel, from the unions the kernel used
     long long starts = 0, fma = 0;
-    for (long long b = 0; b < nbatch; ++b) {
-      long long np_b = std::min<long long>(batch, np - b * batch);
-      for (int u = 0; u < hc[b]; ++u) {
-        int dd = hl[(size_t)b * D + u];
-        long long s = hskip[dd];
-        long long js = (n + s - 1) / s;
-        starts += np_b * js;
-        fma += np_b * js * 2LL * hw[dd];
+    for (int c = 0; c < n_curves; ++c) {
+      const CurveDev<Real>& C = cd[c];
+      std::vector<int> hc(C.nbatch), hl((size_t)C.nbatch * C.D);
+      GTLS_TRY_CUDA(ctx, cudaMemcpy(hc.data(), C.union_cnt, sizeof(int) * C.nbatch, cudaMemcpyDeviceToHost));
+      GTLS_TRY_CUDA(ctx, cudaMemcpy(hl.data(), C.union_list, sizeof(int) * hl.size(), cudaMemcpyDeviceToHost));
+      for (long long b = 0; b < C.nbatch; ++b) {
+        long long np_b = std::min<long long>(C.batch, C.np - b * C.batch);
+        for (int u = 0; u < hc[b]; ++u) {
+          int dd = hl[(size_t)b * C.D + u];
+          long long sk = hskip[c][dd];
+          long long js = (C.n + sk - 1) / sk;
+          starts += np_b * js;
+          fma += np_b * js * 2LL * hw[c][dd];
+        }
       }
     }
     tm->chi2_starts = starts;
@@ -1163,6 +1360,17 @@ static int run_search(gtls_ctx* ctx, const gtls_search_desc* d, cudaStream_t st)
   return GTLS_OK;
 }
 
+static int check_curve(gtls_ctx* ctx, const CurveHost& h) {
+  if (h.n < 2 || !h.t || !h.y || !h.dy || (h.np > 0 && !h.periods) || !h.widths || !h.overshoot || !h.templates ||
+      (h.np > 0 && !h.chi2_out))
+    return fail(ctx, GTLS_E_INVALID, "null pointer or fewer than 2 samples");
+  if (h.np < 0 || h.D < 1 || h.D > GTLS_MAX_DURATIONS)
+    return fail(ctx, GTLS_E_INVALID, "n_periods >= 0 and 1 <= n_durations <= GTLS_MAX_DURATIONS required");
+  if (h.max_width < 1 || h.max_width > h.n) return fail(ctx, GTLS_E_INVALID, "max_width must be in [1, n]");
+  if (h.batch < 1) return fail(ctx, GTLS_E_INVALID, "batch must be >= 1");
+  return GTLS_OK;
+}
+
 }  // namespace gtls
 
 using namespace gtls;
@@ -1170,20 +1378,74 @@ using namespace gtls;
 extern "C" int gtls_search(gtls_ctx* ctx, const gtls_search_desc* d, void* stream) {
   if (!ctx) return GTLS_E_INVALID;
   if (!d || d->abi_version != GTLS_ABI_VERSION) return fail(ctx, GTLS_E_INVALID, "bad descriptor or ABI version");
-  if (d->n < 2 || !d->t || !d->y || !d->dy || !d->periods || !d->widths || !d->overshoot || !d->templates ||
-      !d->chi2_out)
-    return fail(ctx, GTLS_E_INVALID, "null pointer or fewer than 2 samples");
-  if (d->n_periods < 1 || d->n_durations < 1 || d->n_durations > GTLS_MAX_DURATIONS)
-    return fail(ctx, GTLS_E_INVALID, "n_periods >= 1 and 1 <= n_durations <= GTLS_MAX_DURATIONS required");
-  if (d->max_width < 1 || d->max_width > d->n)
-    return fail(ctx, GTLS_E_INVALID, "max_width must be in [1, n]");
-  if (d->batch < 1 || d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "batch and skip_point must be >= 1");
+  if (d->n_periods < 1) return fail(ctx, GTLS_E_INVALID, "n_periods >= 1 required");
+  if (d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "skip_point must be >= 1");
   if (d->pass != GTLS_PASS_MAIN && d->pass != GTLS_PASS_ALL) return fail(ctx, GTLS_E_INVALID, "unknown pass");
-  if ((long long)d->n * d->n_durations >= (1LL << 62)) return fail(ctx, GTLS_E_RANGE, "index overflow");
+  CurveHost h;
+  h.t = d->t;
+  h.y = d->y;
+  h.dy = d->dy;
+  h.periods = d->periods;
+  h.chi2_out = d->chi2_out;
+  h.loc_out = d->loc_out;
+  h.widths = d->widths;
+  h.overshoot = d->overshoot;
+  h.templates = d->templates;
+  h.np = d->n_periods;
+  h.n = d->n;
+  h.D = d->n_durations;
+  h.max_width = d->max_width;
+  h.batch = d->batch;
+  h.span = d->span;
+  int rc = check_curve(ctx, h);
+  if (rc) return rc;
   GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (d->precision == GTLS_FP64) return run_search<double>(ctx, d, st);
-  if (d->precision == GTLS_FP32) return run_search<float>(ctx, d, st);
+  if (d->precision == GTLS_FP64) return run_search<double>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->timing, st);
+  if (d->precision == GTLS_FP32) return run_search<float>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->timing, st);
+  return fail(ctx, GTLS_E_INVALID, "unknown precision");
+}
+
+extern "C" int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* d, void* stream) {
+  if (!ctx) return GTLS_E_INVALID;
+  if (!d || d->abi_version != GTLS_ABI_VERSION) return fail(ctx, GTLS_E_INVALID, "bad descriptor or ABI version");
+  if (d->n_curves < 1 || !d->sample_off || !d->period_off || !d->dur_off || !d->tmpl_off || !d->max_width ||
+      !d->batch || !d->span)
+    return fail(ctx, GTLS_E_INVALID, "null host array or no curves");
+  if (d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "skip_point must be >= 1");
+  if (d->pass != GTLS_PASS_MAIN && d->pass != GTLS_PASS_ALL) return fail(ctx, GTLS_E_INVALID, "unknown pass");
+  std::vector<CurveHost> hs(d->n_curves);
+  for (int c = 0; c < d->n_curves; ++c) {
+    CurveHost& h = hs[c];
+    const long long s0 = d->sample_off[c], s1 = d->sample_off[c + 1];
+    const long long p0 = d->period_off[c], p1 = d->period_off[c + 1];
+    const long long q0 = d->dur_off[c], q1 = d->dur_off[c + 1];
+    if (s1 - s0 > (1LL << 30) || s1 < s0 || p1 < p0 || q1 <= q0)
+      return fail(ctx, GTLS_E_INVALID, "offsets must be non-decreasing (every curve needs a duration)");
+    h.t = d->t + s0;
+    h.y = d->y + s0;
+    h.dy = d->dy + s0;
+    h.periods = d->periods + p0;
+    h.chi2_out = d->chi2_out + p0;
+    h.loc_out = d->loc_out ? d->loc_out + p0 : nullptr;
+    h.widths = d->widths + q0;
+    h.overshoot = d->overshoot + q0;
+    h.templates = d->templates + d->tmpl_off[c];
+    h.np = p1 - p0;
+    h.n = (int)(s1 - s0);
+    h.D = (int)(q1 - q0);
+    h.max_width = d->max_width[c];
+    h.batch = d->batch[c];
+    h.span = d->span[c];
+    int rc = check_curve(ctx, h);
+    if (rc) return rc;
+  }
+  GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (d->precision == GTLS_FP64)
+    return run_search<double>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->timing, st);
+  if (d->precision == GTLS_FP32)
+    return run_search<float>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->timing, st);
   return fail(ctx, GTLS_E_INVALID, "unknown precision");
 }
 
@@ -1197,6 +1459,7 @@ extern "C" int gtls_duration_ranges(gtls_ctx* ctx, const double* periods, int64_
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   duration_range_kernel<<<(unsigned)((n_periods + 255) / 256), 256, 0, st>>>(periods, n_periods, span, n_samples,
                                                                              wmin, wmax);
+  ctx->launches += 1;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
   return GTLS_OK;
 }

@@ -42,10 +42,31 @@ def transit_flux(t, per, rp, a, inc, ecc, w, u, limb_dark):
     return ldmodel.light_curve(t, 0.0, per, rp, a, inc, u)
 
 
+_FLUX_CACHE = {}
+
+
+def _supersampled_flux(per, rp, a, inc, ecc, w, u, limb_dark):
+    """Flux of the reference planet on the SUPERSAMPLE_SIZE grid over one day.
+
+    It depends only on the planet parameters, so a batch of light curves
+    sharing them computes it once (the occultation integral dominates the
+    cost of a template set)."""
+    key = (float(per), float(rp), float(a), float(inc), float(ecc), float(w),
+           tuple(float(v) for v in np.atleast_1d(u)), str(limb_dark))
+    hit = _FLUX_CACHE.get(key)
+    if hit is None:
+        t = np.linspace(-0.5, 0.5, constants.SUPERSAMPLE_SIZE)
+        flux = transit_flux(t, per, rp, a, inc, ecc, w, u, limb_dark)
+        flux.setflags(write=False)
+        if len(_FLUX_CACHE) > 64:
+            _FLUX_CACHE.clear()
+        hit = _FLUX_CACHE[key] = (t, flux)
+    return hit
+
+
 def reference_transit(samples, per, rp, a, inc, ecc, w, u, limb_dark):
     """Unit-width, unit-depth reference transit on ``samples`` points (transit.py:8-42)."""
-    t = np.linspace(-0.5, 0.5, constants.SUPERSAMPLE_SIZE)
-    flux = transit_flux(t, per, rp, a, inc, ecc, w, u, limb_dark)
+    t, flux = _supersampled_flux(per, rp, a, inc, ecc, w, u, limb_dark)
     idx_first = int(np.argmax(flux < 1))
     intransit_flux = flux[idx_first: -idx_first + 1]
     intransit_time = t[idx_first: -idx_first + 1]

@@ -61,6 +61,13 @@ int gtls_abi_version(void);
  * (no counterpart in the reference; used to account for device work). */
 int64_t gtls_launch_count(const gtls_ctx* ctx);
 
+/* Bytes of per-chunk scratch a search may use (fold records, prefix sums,
+ * sort slots; default 8 GiB).  Periods are processed in chunks that fit it;
+ * results do not depend on it.  No counterpart in the reference, whose
+ * batch size comes from the free-memory formula of core.py:620-628.
+ * bytes must be >= 1 MiB. */
+int gtls_set_chunk_budget(gtls_ctx* ctx, uint64_t bytes);
+
 /*
  * Ofir-optimal period grid, evaluated on the device.
  * Replaces the per-point part of grid.period_grid (grid.py:126-137):
@@ -143,6 +150,49 @@ typedef struct gtls_search_desc {
 #define GTLS_MAX_DURATIONS 1024
 
 int gtls_search(gtls_ctx* ctx, const gtls_search_desc* desc, void* stream);
+
+/*
+ * Many light curves searched in one call (the batched survey case: one
+ * independent search per curve, as a loop of gtls_search calls would do, with
+ * the prepare/chi2/finish launches shared by all curves).  No counterpart in
+ * the reference, which searches one curve per gtls() object.  Curve c owns
+ *   samples   [sample_off[c], sample_off[c+1])  of t, y, dy
+ *   periods   [period_off[c], period_off[c+1])  of periods, chi2_out, loc_out
+ *   durations [dur_off[c], dur_off[c+1])        of widths, overshoot
+ *   templates starting at tmpl_off[c], (dur_off[c+1]-dur_off[c]) * max_width[c] values
+ * and its own max_width, batch and span (host arrays of n_curves values);
+ * offsets are host arrays of n_curves + 1 values.  Results per curve are the
+ * ones gtls_search gives for that curve alone.  timing, when non-NULL, sums
+ * over all curves.
+ */
+typedef struct gtls_batch_desc {
+  int32_t abi_version;        /* GTLS_ABI_VERSION                               */
+  int32_t precision;          /* gtls_precision                                 */
+  int32_t pass;               /* gtls_pass                                      */
+  int32_t n_curves;
+  const int64_t* sample_off;  /* host [n_curves + 1]                            */
+  const int64_t* period_off;  /* host [n_curves + 1]                            */
+  const int64_t* dur_off;     /* host [n_curves + 1]                            */
+  const int64_t* tmpl_off;    /* host [n_curves]                                */
+  const int32_t* max_width;   /* host [n_curves]                                */
+  const int32_t* batch;       /* host [n_curves]                                */
+  const float* span;          /* host [n_curves]                                */
+  const double* t;            /* device, all curves' samples                    */
+  const double* y;
+  const double* dy;
+  const double* periods;      /* device, all curves' periods                    */
+  const int32_t* widths;      /* device, all curves' durations                  */
+  const double* overshoot;
+  const double* templates;    /* device, all curves' template rows              */
+  double depth_min;
+  int32_t skip_point;
+  int32_t reserved;
+  double* chi2_out;           /* device, all curves' periods                    */
+  int64_t* loc_out;           /* device or NULL                                 */
+  gtls_timing* timing;        /* host, or NULL                                  */
+} gtls_batch_desc;
+
+int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* desc, void* stream);
 
 /*
  * Spectra of a chi2 array (stats.spectra, stats.py:95-122, with the

@@ -33,3 +33,32 @@ def test_context_creation_reports_errors_without_a_gpu():
     rc = lib.gtls_ctx_create(0, ctypes.byref(h))
     assert rc != 0
     assert len(lib.gtls_last_error(None)) > 0
+
+
+def test_ctypes_descriptors_match_the_c_layout(tmp_path):
+    """Size and field offsets of the ctypes mirrors equal the C compiler's."""
+    import shutil
+    import subprocess
+    from gtls_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    structs = {"gtls_search_desc": _lib.SearchDesc, "gtls_batch_desc": _lib.BatchDesc, "gtls_timing": _lib.Timing}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtls_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in py._fields_:
+            cf = "pass" if fname == "pass_" else fname
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, cf))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
