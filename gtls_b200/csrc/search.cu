@@ -710,6 +710,18 @@ __device__ __forceinline__ Real warp_reduce_scatter18(const Real (&aB)[kR], cons
   return v[0];
 }
 
+// Dynamic shared memory of one chi2 CTA: the record tile (rounded up to 16
+// bytes) followed by the per-duration table (overshoot, width | skip << 16,
+// template row offset).
+template <typename Real>
+__host__ __device__ __forceinline__ size_t chi2_tile_bytes(int tile, int maxd) {
+  return ((size_t)(tile + maxd) * sizeof(typename Tr<Real>::R2) + 15) & ~(size_t)15;
+}
+template <typename Real>
+__host__ __device__ __forceinline__ size_t chi2_smem_bytes(int tile, int maxd, int D) {
+  return chi2_tile_bytes<Real>(tile, maxd) + (size_t)D * (sizeof(Real) + 2 * sizeof(int));
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kChiThreads, 1)
 chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs,
@@ -748,6 +760,17 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   const double sentinel = (double)n;
   const int* __restrict__ skips = C.skips;
   const int lane = threadIdx.x & 31;
+  // per-duration table after the tile: overshoot, (width | skip << 16), template row offset
+  Real* dtab_os = reinterpret_cast<Real*>(smem_raw + chi2_tile_bytes<Real>(C.tile, C.maxd));
+  int* dtab_ws = reinterpret_cast<int*>(dtab_os + D);
+  int* dtab_row = dtab_ws + D;
+  const R2* __restrict__ trows = C.trows;
+  if (threadIdx.x >= 32)
+    for (int d = (int)threadIdx.x - 32; d < D; d += (int)blockDim.x - 32) {
+      dtab_os[d] = (Real)C.overshoot[d];
+      dtab_ws[d] = C.widths[d] | (skips[d] << 16);
+      dtab_row[d] = C.trow_off[d];
+    }
 
   // stage the records [k0, k0 + L) in shared memory with one bulk (TMA) copy;
   // the byte count is rounded up to 16 (the record rows are padded for it)
@@ -817,13 +840,14 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     const int sub = tk - task_pre[u];
     const int upos = task_dur[u];        // position in ascending union order
     const int d = ulist[upos];
-    const int w = C.widths[d];
-    const int s = skips[d];
+    const int ws = dtab_ws[d];
+    const int w = ws & 0xffff;
+    const int s = ws >> 16;
     const int Q = (w + s - 1) / s;
     const int jlo = (k0 + s - 1) / s;
     const int jhi = (k1 + s - 1) / s;
-    const R2* trow = C.trows + C.trow_off[d];
-    const Real os = (Real)C.overshoot[d];
+    const R2* trow = trows + dtab_row[d];
+    const Real os = dtab_os[d];
     const Real inv_w = (Real)1 / (Real)w;
     const long long locb = (long long)upos * n;
     Real aB[kR], aC[kR];
@@ -1087,7 +1111,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
       hlen[c][i] = (Qr + 1) * sk;   // one extra zero block: the one-step template prefetch reads it
       rows += hlen[c][i];
     }
-    long long tile = ((long long)(smem_budget / sizeof(R2)) - maxd) / 256 * 256;
+    if (maxd > 0xffff) return fail(ctx, GTLS_E_RANGE, "max_width above 65535");
+    const size_t table = (size_t)D * (sizeof(Real) + 2 * sizeof(int)) + 16;
+    long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd) / 256 * 256;
     if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
     tile = std::min<long long>(tile, 8192);
     if (tile > n) tile = (n + 255) / 256 * 256;
@@ -1187,7 +1213,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
         items += (int)take;
         tiles += (int)(take * C.ntiles);
         sm_prep = std::max(sm_prep, sizeof(int) << C.nb_log2);
-        sm_chi = std::max(sm_chi, (size_t)(C.tile + C.maxd) * sizeof(R2));
+        sm_chi = std::max(sm_chi, chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
         p += take;
       }
     }
