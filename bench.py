@@ -40,7 +40,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
+                    help="main-pass precision (default: fp32 for cfg4, fp64 otherwise)")
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--curves", type=int, default=32,
                     help="cfg4: curves per step (every 4096/curves-th curve of the 4,096-curve set)")
@@ -504,6 +505,8 @@ def bench_cfg3(args):
 
 def main():
     args = parse()
+    if args.precision is None:
+        args.precision = "fp32" if args.workload == "cfg4" else "fp64"
     if args.chunk_mb and args.impl == "ours":
         from gtls_b200 import _lib
         import torch

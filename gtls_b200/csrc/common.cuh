@@ -5,7 +5,7 @@
 #include <cstdint>
 #include <string>
 
-#include "../../include/gtls_b200.h"
+#include "gtls_b200.h"
 
 struct gtls_ctx {
   int device = 0;

@@ -50,6 +50,8 @@
 namespace gtls {
 
 constexpr int kPrepThreads = 1024;
+constexpr int kSmallBucket = 8;     // entries of buckets up to this size are ranked by their own thread
+constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (warp-ranked)
 constexpr int kChiThreads = 512;
 constexpr int kR = 9;            // starts per register block (odd: conflict-free strides)
 constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset rho
@@ -60,6 +62,7 @@ template <> struct Tr<double> {
   using R2 = double2;   // (u, w) record / (s, s^2) template pair
   using Pv = double;    // prefix of v
 };
+static_assert(sizeof(float2) == sizeof(double), "float-float prefix shares the FP64 slot");
 template <> struct Tr<float> {
   using R2 = float2;
   using Pv = float2;    // (hi, lo) float-float prefix of v
@@ -77,6 +80,19 @@ __device__ __forceinline__ float2 ff_add(float2 a, float2 b) {
 __device__ __forceinline__ float2 ff_from_double(double v) {
   float hi = (float)v;
   return make_float2(hi, (float)(v - (double)hi));
+}
+// Store prefix value v at pre[r] through the FP64 view of the prefix array:
+// as a double (FP64 form) or as the float-float pair (hi, lo) occupying the
+// same 8 bytes (FP32 form; hi at the lower address).
+template <typename Real>
+__device__ __forceinline__ void store_prefix(double* pre, int r, double v) {
+  if constexpr (sizeof(Real) == 8) {
+    pre[r] = v;
+  } else {
+    const float2 f = ff_from_double(v);
+    const unsigned long long bits = ((unsigned long long)__float_as_uint(f.y) << 32) | __float_as_uint(f.x);
+    pre[r] = __longlong_as_double((long long)bits);
+  }
 }
 
 // ------------------------------------------------------------ descriptors
@@ -167,106 +183,40 @@ __global__ void __launch_bounds__(1024) curve_setup_kernel(const CurveDev<Real>*
 }
 
 // ------------------------------------------------------------ block scans
-// Exclusive scan of an int array in shared memory, in place; returns total.
+// Exclusive scan of an int array in shared memory, in place; returns the
+// total.  Warp w owns the contiguous range [w*per, (w+1)*per) and walks it 32
+// consecutive entries at a time, so that lanes never share a bank.
 __device__ int block_exclusive_scan_smem(int* a, int len, int* warp_tmp) {
-  const int per = (len + blockDim.x - 1) / blockDim.x;
-  const int beg = min(len, (int)threadIdx.x * per);
-  const int end = min(len, beg + per);
-  int local = 0;
-  for (int i = beg; i < end; ++i) local += a[i];
-  // block exclusive scan of `local`
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int x = local;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int per = ((len + nw - 1) / nw + 31) & ~31;
+  const int beg = min(len, wid * per), end = min(len, beg + per);
+  int sum = 0;
+  for (int i = beg + lane; i < end; i += 32) sum += a[i];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int yv = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += yv;
-  }
-  if (lane == 31) warp_tmp[wid] = x;
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) warp_tmp[wid] = sum;
   __syncthreads();
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    int z = lane < nw ? warp_tmp[lane] : 0;
+  int carry = lane < wid ? warp_tmp[lane] : 0;
+  int total = lane < nw ? warp_tmp[lane] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    carry += __shfl_xor_sync(0xffffffffu, carry, o);
+    total += __shfl_xor_sync(0xffffffffu, total, o);
+  }
+  for (int i0 = beg; i0 < end; i0 += 32) {
+    const int i = i0 + lane;
+    const int x = i < end ? a[i] : 0;
+    int inc = x;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int yv = __shfl_up_sync(0xffffffffu, z, o);
-      if (lane >= o) z += yv;
+      const int yv = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += yv;
     }
-    if (lane < nw) warp_tmp[lane] = z;  // inclusive warp totals
-  }
-  __syncthreads();
-  int total = warp_tmp[(blockDim.x >> 5) - 1];
-  int run = x - local + (wid > 0 ? warp_tmp[wid - 1] : 0);
-  for (int i = beg; i < end; ++i) {
-    int c = a[i];
-    a[i] = run;
-    run += c;
+    if (i < end) a[i] = carry + inc - x;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
   }
   __syncthreads();
   return total;
-}
-
-// Exclusive block scan of one double per thread (fixed order, deterministic).
-__device__ double block_exclusive_scan_double(double x, double* warp_tmp, double* total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double yv = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += yv;
-  }
-  if (lane == 31) warp_tmp[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    double z = lane < nw ? warp_tmp[lane] : 0.0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      double yv = __shfl_up_sync(0xffffffffu, z, o);
-      if (lane >= o) z += yv;
-    }
-    if (lane < nw) warp_tmp[lane] = z;
-  }
-  __syncthreads();
-  *total = warp_tmp[(blockDim.x >> 5) - 1];
-  double r = inc - x + (wid > 0 ? warp_tmp[wid - 1] : 0.0);
-  __syncthreads();
-  return r;
-}
-
-__device__ float2 block_exclusive_scan_ff(float2 x, float2* warp_tmp) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  float2 inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    float2 yv;
-    yv.x = __shfl_up_sync(0xffffffffu, inc.x, o);
-    yv.y = __shfl_up_sync(0xffffffffu, inc.y, o);
-    if (lane >= o) inc = ff_add(yv, inc);
-  }
-  if (lane == 31) warp_tmp[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    float2 z = lane < nw ? warp_tmp[lane] : make_float2(0.f, 0.f);
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      float2 yv;
-      yv.x = __shfl_up_sync(0xffffffffu, z.x, o);
-      yv.y = __shfl_up_sync(0xffffffffu, z.y, o);
-      if (lane >= o) z = ff_add(yv, z);
-    }
-    if (lane < nw) warp_tmp[lane] = z;
-  }
-  __syncthreads();
-  // exclusive = (warp prefix before this warp) + (inclusive - x) recomputed as a scan shift
-  float2 prev = (wid > 0) ? warp_tmp[wid - 1] : make_float2(0.f, 0.f);
-  float2 lanex;
-  lanex.x = __shfl_up_sync(0xffffffffu, inc.x, 1);
-  lanex.y = __shfl_up_sync(0xffffffffu, inc.y, 1);
-  float2 r = (lane == 0) ? prev : ff_add(prev, lanex);
-  __syncthreads();
-  return r;
 }
 
 // ---------------------------------------------------------------- prepare
@@ -299,6 +249,32 @@ __device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __rest
   return a.y < b.y;
 }
 
+// Rank of every entry of bucket slots [s, e) among the bucket (ord[s + rank] =
+// original index), by a whole warp: each lane ranks one entry of a group of
+// 32 against the bucket, streamed 32 entries at a time and broadcast by
+// shuffles.  Used for large buckets, whose O(k^2) comparisons would
+// otherwise fall on single threads.
+__device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot, int* __restrict__ ord, int s, int e,
+                                                 const double* __restrict__ t, double P) {
+  const int lane = threadIdx.x & 31;
+  for (int j0 = s; j0 < e; j0 += 32) {
+    const int j = j0 + lane;
+    const uint2 mine = slot[min(j, e - 1)];
+    int r = 0;
+    for (int m0 = s; m0 < e; m0 += 32) {
+      const uint2 oth = slot[min(m0 + lane, e - 1)];
+      const int cnt = min(32, e - m0);
+      for (int q = 0; q < cnt; ++q) {
+        uint2 o;
+        o.x = __shfl_sync(0xffffffffu, oth.x, q);
+        o.y = __shfl_sync(0xffffffffu, oth.y, q);
+        if (o.y != mine.y && slot_less(o, mine, t, P)) ++r;
+      }
+    }
+    if (j < e) ord[s + r] = (int)mine.y;
+  }
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kPrepThreads)
 prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
@@ -308,7 +284,9 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   using Pv = typename Tr<Real>::Pv;
   extern __shared__ int hist[];
   __shared__ int wtmp_i[32];
-  __shared__ Pv wsum[32];
+  __shared__ double wsum[32];
+  __shared__ int big[kBigBuckets];
+  __shared__ int nbig;
   const int item = blockIdx.x;
   const int ri = upper_find(0, nruns, item, [&](int i) { return (long long)runs[i].item0; });
   const Run& R = runs[ri];
@@ -327,10 +305,12 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   int* ord = scr_ord + R.slot_off + (size_t)local * n;
   R2* out = rec + R.rec_off + (size_t)local * Mrec;
   Pv* pre = pv + R.pv_off + (size_t)local * (M + 1);
+  double* pre_d = reinterpret_cast<double*>(pre);   // FP64 view during the scan (Pv is 8 bytes)
   constexpr int kB = 4;   // elements per thread in flight in each pass
   const int stride = blockDim.x * kB;
 
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
+  if (threadIdx.x == 0) nbig = 0;
   __syncthreads();
   // (1) fold and histogram of buckets
   for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
@@ -370,19 +350,49 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
     }
   }
   __syncthreads();
-  // (3) each thread ranks whole buckets: ord[start + rank] = original index
+  // (3) ranking within buckets: ord[start + rank] = original index.
+  //     (a) buckets of more than kSmallBucket entries (clustered phases, as
+  //         when the period is close to a multiple of a regular cadence) are
+  //         listed, from the shared-memory counts alone;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    const int s = b == 0 ? 0 : hist[b - 1];
-    const int e = hist[b];
-    if (e - s == 1) {
-      ord[s] = (int)slot[s].y;
-    } else if (e - s > 1) {
-      for (int j = s; j < e; ++j) {
+    const int k = hist[b] - (b == 0 ? 0 : hist[b - 1]);
+    if (k > kSmallBucket) {
+      const int q = atomicAdd(&nbig, 1);
+      if (q < kBigBuckets) big[q] = b;
+    }
+  }
+  __syncthreads();
+  //     (b) whole warps rank the listed buckets (unless the list overflowed);
+  const bool warp_ranked = nbig <= kBigBuckets;
+  if (warp_ranked)
+    for (int q = (int)(threadIdx.x >> 5); q < nbig; q += (int)(blockDim.x >> 5)) {
+      const int b = big[q];
+      rank_bucket_warp(slot, ord, b == 0 ? 0 : hist[b - 1], hist[b], t, P);
+    }
+  //     (c) every other entry is ranked by its own thread: coalesced over the
+  //         slots, its bucket found by binary search of the bucket ends.
+  for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int j = i0 + u * blockDim.x;
+      if (j < n) {
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (hist[mid] > j) hi = mid;
+          else lo = mid + 1;
+        }
+        const int s = lo == 0 ? 0 : hist[lo - 1];
+        const int e = hist[lo];
         const uint2 sj = slot[j];
-        int r = 0;
-        for (int m = s; m < e; ++m)
-          if (m != j) r += slot_less(slot[m], sj, t, P);
-        ord[s + r] = (int)sj.y;
+        if (e - s == 1) {
+          ord[j] = (int)sj.y;
+        } else if (e - s <= kSmallBucket || !warp_ranked) {
+          int r = 0;
+          for (int m = s; m < e; ++m)
+            if (m != j) r += slot_less(slot[m], sj, t, P);
+          ord[s + r] = (int)sj.y;
+        }
       }
     }
   }
@@ -409,70 +419,38 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
         o.x = (Real)(g[u].x * g[u].y);
         o.y = (Real)g[u].y;
         out[r] = o;
-        if constexpr (sizeof(Real) == 8) pre[r + 1] = g[u].x;
-        else pre[r + 1] = ff_from_double(g[u].x);
+        pre_d[r + 1] = g[u].x;
       }
     }
   }
   __syncthreads();
-  // (5) prefix of v in place over pre[1..M]: each warp scans a contiguous
-  //     range (coalesced), then adds the sum of the ranges before it
+  // (5) prefix of v in place over pre[1..M], accumulated in FP64 for both
+  //     forms (the FP32 form then stores each prefix as a float-float pair
+  //     (hi, lo) in the same 8 bytes): each warp scans a contiguous range
+  //     (coalesced), then adds the sum of the ranges before it
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int per = (M + nwarp - 1) / nwarp;
   const int beg = 1 + min(M, wid * per);
   const int end = 1 + min(M, (wid + 1) * per);
-  if constexpr (sizeof(Real) == 8) {
-    double acc = 0.0;
-    for (int r = beg + lane; r < end; r += 32) acc += pre[r];
+  double acc = 0.0;
+  for (int r = beg + lane; r < end; r += 32) acc += pre_d[r];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) wsum[wid] = acc;
-    __syncthreads();
-    double carry = 0.0;
-    for (int w = 0; w < wid; ++w) carry += wsum[w];
-    if (wid == 0 && lane == 0) pre[0] = 0.0;
-    for (int r0 = beg; r0 < end; r0 += 32) {
-      const int r = r0 + lane;
-      double x = r < end ? pre[r] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) wsum[wid] = acc;
+  __syncthreads();
+  double carry = 0.0;
+  for (int w = 0; w < wid; ++w) carry += wsum[w];
+  if (wid == 0 && lane == 0) store_prefix<Real>(pre_d, 0, 0.0);
+  for (int r0 = beg; r0 < end; r0 += 32) {
+    const int r = r0 + lane;
+    double x = r < end ? pre_d[r] : 0.0;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        double yv = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += yv;
-      }
-      if (r < end) pre[r] = carry + x;
-      carry += __shfl_sync(0xffffffffu, x, 31);
+    for (int o = 1; o < 32; o <<= 1) {
+      const double yv = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += yv;
     }
-  } else {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int r = beg + lane; r < end; r += 32) acc = ff_add(acc, pre[r]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      float2 yv;
-      yv.x = __shfl_xor_sync(0xffffffffu, acc.x, o);
-      yv.y = __shfl_xor_sync(0xffffffffu, acc.y, o);
-      acc = ff_add(acc, yv);
-    }
-    if (lane == 0) wsum[wid] = acc;
-    __syncthreads();
-    float2 carry = make_float2(0.f, 0.f);
-    for (int w = 0; w < wid; ++w) carry = ff_add(carry, wsum[w]);
-    if (wid == 0 && lane == 0) pre[0] = make_float2(0.f, 0.f);
-    for (int r0 = beg; r0 < end; r0 += 32) {
-      const int r = r0 + lane;
-      float2 x = r < end ? pre[r] : make_float2(0.f, 0.f);
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        float2 yv;
-        yv.x = __shfl_up_sync(0xffffffffu, x.x, o);
-        yv.y = __shfl_up_sync(0xffffffffu, x.y, o);
-        if (lane >= o) x = ff_add(yv, x);
-      }
-      if (r < end) pre[r] = ff_add(carry, x);
-      float2 tot;
-      tot.x = __shfl_sync(0xffffffffu, x.x, 31);
-      tot.y = __shfl_sync(0xffffffffu, x.y, 31);
-      carry = ff_add(carry, tot);
-    }
+    if (r < end) store_prefix<Real>(pre_d, r, carry + x);
+    carry += __shfl_sync(0xffffffffu, x, 31);
   }
 }
 
