@@ -55,6 +55,10 @@ constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (w
 constexpr int kChiThreads = 512;
 constexpr int kR = 9;            // starts per register block (odd: conflict-free strides)
 constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset rho
+// Zeroed records after each shared-memory tile: a skip-1 group whose kR
+// starts all lie in the tile reads at most kR - 2 records past it (only ever
+// against zero template entries), so those groups need no clamping.
+constexpr int kTilePad = 16;
 
 // ---------------------------------------------------------------- precision
 template <typename Real> struct Tr;
@@ -561,6 +565,54 @@ __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restric
   }
 }
 
+// correlate() for skip 1 (every start: the all-starts pass and widths up to
+// the skip point) and a group whose kR starts all lie in the tile: no
+// clamping (the reads stay inside the tile and its zeroed pad), whole blocks
+// of kR template entries (entries past Q are zero), consecutive records and
+// template entries addressed with constant offsets from block pointers.  The FP32 form adds each block of kR
+// products to the running sums separately (two-level summation).
+template <typename Real, bool kTwoLevel>
+__device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __restrict__ tile, int base,
+                                             const typename Tr<Real>::R2* __restrict__ trow, int Qr,
+                                             Real (&aB)[kR], Real (&aC)[kR]) {
+  using R2 = typename Tr<Real>::R2;
+  R2 xs[kR];
+  const R2* xp = tile + base;
+#pragma unroll
+  for (int i = 0; i < kR - 1; ++i) xs[i] = xp[i];
+  for (int q0 = 0; q0 < Qr; q0 += kR) {
+    Real pB[kR], pC[kR];
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      pB[r] = kTwoLevel ? (Real)0 : aB[r];
+      pC[r] = kTwoLevel ? (Real)0 : aC[r];
+    }
+    const R2* xb = xp + q0 + kR - 1;
+    const R2* tb = trow + q0;
+#pragma unroll
+    for (int qq = 0; qq < kR; ++qq) {
+      xs[(qq + kR - 1) % kR] = xb[qq];
+      const R2 tq = tb[qq];
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        const R2 x = xs[(qq + r) % kR];
+        pB[r] = fma(tq.x, x.x, pB[r]);
+        pC[r] = fma(tq.y, x.y, pC[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      if (kTwoLevel) {
+        aB[r] += pB[r];
+        aC[r] += pC[r];
+      } else {
+        aB[r] = pB[r];
+        aC[r] = pC[r];
+      }
+    }
+  }
+}
+
 // Same sums for the lanes-split path: the kR template entries of one block of
 // kR template offsets are loaded together first (kR loads in flight), then the
 // 2*kR-1 records they touch stream through once.
@@ -693,14 +745,17 @@ __device__ __forceinline__ Real warp_reduce_scatter18(const Real (&aB)[kR], cons
 // template row offset).
 template <typename Real>
 __host__ __device__ __forceinline__ size_t chi2_tile_bytes(int tile, int maxd) {
-  return ((size_t)(tile + maxd) * sizeof(typename Tr<Real>::R2) + 15) & ~(size_t)15;
+  return ((size_t)(tile + maxd + kTilePad) * sizeof(typename Tr<Real>::R2) + 15) & ~(size_t)15;
 }
 template <typename Real>
 __host__ __device__ __forceinline__ size_t chi2_smem_bytes(int tile, int maxd, int D) {
   return chi2_tile_bytes<Real>(tile, maxd) + (size_t)D * (sizeof(Real) + 2 * sizeof(int));
 }
 
-template <typename Real>
+// kAllStarts: the instance for the all-starts pass (every skip is 1), which
+// alone carries the unclamped skip-1 path, so that the main-pass instance
+// keeps its register allocation.
+template <typename Real, bool kAllStarts>
 __global__ void __launch_bounds__(kChiThreads, 1)
 chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs,
             const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Real>::Pv* __restrict__ pv,
@@ -791,6 +846,15 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     }
   }
   __syncthreads();
+  // zero the pad after the tile's L records (the copy's rounding to 16 bytes
+  // may have brought in one record past them, possibly an unwritten one)
+  for (int i = L + (int)threadIdx.x; i < L + kTilePad; i += blockDim.x) {
+    R2 zr;
+    zr.x = (Real)0;
+    zr.y = (Real)0;
+    tile[i] = zr;
+  }
+  __syncthreads();
 
   Best best{INFINITY, 0x7fffffffffffffffLL};
   // the first start skipped by k % skip != 0 carries the value n (GPUFun.py:407,409)
@@ -858,8 +922,13 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       // each lane takes kR consecutive start blocks and every rho
       const int jb = jlo + (sub * 32 + lane) * kR;
       if (jb < jhi) {
-        for (int rho = 0; rho < s; ++rho)
-          correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+        const int Qr = (Q + kR - 1) / kR * kR;
+        if (kAllStarts && s == 1 && jb + kR <= jhi) {
+          correlate_s1<Real, kTwoLevel>(tile, jb - k0, trow, Qr, aB, aC);
+        } else {
+          for (int rho = 0; rho < s; ++rho)
+            correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+        }
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const int j = jb + r;
@@ -1091,7 +1160,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     }
     if (maxd > 0xffff) return fail(ctx, GTLS_E_RANGE, "max_width above 65535");
     const size_t table = (size_t)D * (sizeof(Real) + 2 * sizeof(int)) + 16;
-    long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd) / 256 * 256;
+    long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd - kTilePad) / 256 * 256;
     if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
     tile = std::min<long long>(tile, 8192);
     if (tile > n) tile = (n + 255) / 256 * 256;
@@ -1289,7 +1358,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   }
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)std::max<size_t>(max_prep, 1)));
-  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)std::max<size_t>(max_chi, 1)));
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)std::max<size_t>(max_chi, 1)));
   Chi2Args ca;
   ca.pass = precision_pass;
@@ -1309,7 +1380,10 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
                                                                           rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
     ca.nruns = nr;
-    chi2_kernel<Real><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
+    if (all)
+      chi2_kernel<Real, true><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
+    else
+      chi2_kernel<Real, false><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[2], st));
     finish_kernel<Real><<<(items + 127) / 128, 128, 0, st>>>(d_cd, d_runs + r0, nr, items, part_v, part_loc);
     if (tm) {

@@ -84,6 +84,34 @@ def test_other_skip_points_match_oracle(cuda, skip_point):
     np.testing.assert_array_equal(loc.cpu().numpy(), l_ref)
 
 
+@pytest.mark.parametrize("skip_point", [2, 5])
+def test_small_skips_both_precisions_match_oracle(cuda, skip_point):
+    """Skips 1..31 take the lane path: groups whose starts all lie in the tile
+    read unclamped (tile pad), the last group of a tile reads clamped."""
+    from gtls_b200 import _lib
+    s = search_inputs(seed=16, n=1333, span=6.0, use_dy=True)
+    cur = _curve(s)
+    P = s["periods"][::7]
+    c_ref, l_ref = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                    s["overshoot"], s["maxd"], 1e-5, skip_point, 5)
+    for prec, rtol in (("fp64", RTOL64), ("fp32", RTOL32)):
+        chi2, loc = cur.search(P, 1e-5, skip_point, 5, _lib.GTLS_PASS_MAIN, prec, want_loc=True)
+        np.testing.assert_allclose(chi2.cpu().numpy(), c_ref, rtol=rtol)
+        if prec == "fp64":
+            np.testing.assert_array_equal(loc.cpu().numpy(), l_ref)
+
+
+def test_all_starts_pass_fp32_close_to_oracle(cuda):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=17, n=1001, span=5.0)
+    cur = _curve(s)
+    P = s["periods"][::13]
+    chi2, _ = cur.search(P, 1e-5, 8, 4, _lib.GTLS_PASS_ALL, "fp32")
+    c_ref, _ = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                s["overshoot"], s["maxd"], 1e-5, 8, 4, noskip=True)
+    np.testing.assert_allclose(chi2.cpu().numpy(), c_ref, rtol=RTOL32)
+
+
 def test_matches_reference_kernel_fixtures(cuda):
     """Against the reference's own kernels (recorded R64 outputs), per period with its own durations."""
     import torch
