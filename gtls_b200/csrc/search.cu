@@ -509,8 +509,29 @@ __device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::
   }
 }
 
+// (b, c) += (t.x * x.x, t.y * x.y) for an accumulator pair (B, C): one
+// packed two-lane FMA in FP32 (sm_100), two FMAs in FP64.  Same IEEE
+// rounding either way.
+__device__ __forceinline__ void fma_pair(const double2& t, const double2& x, double2& a) {
+  a.x = fma(t.x, x.x, a.x);
+  a.y = fma(t.y, x.y, a.y);
+}
+__device__ __forceinline__ void fma_pair(const float2& t, const float2& x, float2& a) { a = __ffma2_rn(t, x, a); }
+__device__ __forceinline__ void add_pair(double2& a, const double2& b) {
+  a.x += b.x;
+  a.y += b.y;
+}
+__device__ __forceinline__ void add_pair(float2& a, const float2& b) { a = __fadd2_rn(a, b); }
+template <typename R2>
+__device__ __forceinline__ R2 zero_pair() {
+  R2 z;
+  z.x = 0;
+  z.y = 0;
+  return z;
+}
+
 // Correlate template offset rho of kR consecutive starts with the tile:
-//   aB[r] += sum_{q<Q} T[q*s + rho] * u[base + (r+q)*s],  aC[r] likewise with (T^2, w)
+//   acc[r].x (B) += sum_{q<Q} T[q*s + rho] * u[base + (r+q)*s],  acc[r].y (C) likewise with (T^2, w)
 // where base = jb*s + rho - k0 addresses start block jb.  A sliding window of
 // kR records in registers gives one shared-memory load and one template load
 // per kR multiply-add pairs (slot of record q+r is (q+r) % kR; the q loop is
@@ -521,18 +542,15 @@ __device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::
 template <typename Real, bool kTwoLevel>
 __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restrict__ tile, int L, int base, int s,
                                           const typename Tr<Real>::R2* __restrict__ trow, int rho, int Q,
-                                          Real (&aB)[kR], Real (&aC)[kR]) {
+                                          typename Tr<Real>::R2 (&acc)[kR]) {
   using R2 = typename Tr<Real>::R2;
   R2 xs[kR];
   const int last = L - 1;
 #pragma unroll
   for (int i = 0; i < kR - 1; ++i) xs[i] = tile[min(base + i * s, last)];
-  Real pB[kR], pC[kR];
+  R2 pr[kR];
 #pragma unroll
-  for (int r = 0; r < kR; ++r) {
-    pB[r] = kTwoLevel ? (Real)0 : aB[r];
-    pC[r] = kTwoLevel ? (Real)0 : aC[r];
-  }
+  for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
   int pos = base + (kR - 1) * s;
   int toff = rho;
   R2 tnext = trow[toff];
@@ -548,20 +566,16 @@ __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restric
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
         const R2 x = xs[(qq + r) % kR];
-        pB[r] = fma(tq.x, x.x, pB[r]);
-        pC[r] = fma(tq.y, x.y, pC[r]);
+        fma_pair(tq, x, pr[r]);
       }
     }
   }
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    if (kTwoLevel) {
-      aB[r] += pB[r];
-      aC[r] += pC[r];
-    } else {
-      aB[r] = pB[r];
-      aC[r] = pC[r];
-    }
+    if (kTwoLevel)
+      add_pair(acc[r], pr[r]);
+    else
+      acc[r] = pr[r];
   }
 }
 
@@ -569,24 +583,22 @@ __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restric
 // the skip point) and a group whose kR starts all lie in the tile: no
 // clamping (the reads stay inside the tile and its zeroed pad), whole blocks
 // of kR template entries (entries past Q are zero), consecutive records and
-// template entries addressed with constant offsets from block pointers.  The FP32 form adds each block of kR
-// products to the running sums separately (two-level summation).
+// template entries addressed with constant offsets from block pointers.  The
+// FP32 form adds each block of kR products to the running sums separately
+// (two-level summation).
 template <typename Real, bool kTwoLevel>
 __device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __restrict__ tile, int base,
                                              const typename Tr<Real>::R2* __restrict__ trow, int Qr,
-                                             Real (&aB)[kR], Real (&aC)[kR]) {
+                                             typename Tr<Real>::R2 (&acc)[kR]) {
   using R2 = typename Tr<Real>::R2;
   R2 xs[kR];
   const R2* xp = tile + base;
 #pragma unroll
   for (int i = 0; i < kR - 1; ++i) xs[i] = xp[i];
   for (int q0 = 0; q0 < Qr; q0 += kR) {
-    Real pB[kR], pC[kR];
+    R2 pr[kR];
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      pB[r] = kTwoLevel ? (Real)0 : aB[r];
-      pC[r] = kTwoLevel ? (Real)0 : aC[r];
-    }
+    for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
     const R2* xb = xp + q0 + kR - 1;
     const R2* tb = trow + q0;
 #pragma unroll
@@ -596,37 +608,31 @@ __device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __rest
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
         const R2 x = xs[(qq + r) % kR];
-        pB[r] = fma(tq.x, x.x, pB[r]);
-        pC[r] = fma(tq.y, x.y, pC[r]);
+        fma_pair(tq, x, pr[r]);
       }
     }
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-      if (kTwoLevel) {
-        aB[r] += pB[r];
-        aC[r] += pC[r];
-      } else {
-        aB[r] = pB[r];
-        aC[r] = pC[r];
-      }
+      if (kTwoLevel)
+        add_pair(acc[r], pr[r]);
+      else
+        acc[r] = pr[r];
     }
   }
 }
 
 // Same sums for the lanes-split path: the kR template entries of one block of
 // kR template offsets are loaded together first (kR loads in flight), then the
-// 2*kR-1 records they touch stream through once.
-template <typename Real, bool kTwoLevel>
+// 2*kR-1 records they touch stream through once.  kClamp: clamp record reads
+// to the tile (needed only for tasks whose reads may pass its end).
+template <typename Real, bool kTwoLevel, bool kClamp>
 __device__ __forceinline__ void correlate_pre(const typename Tr<Real>::R2* __restrict__ tile, int L, int base,
                                               int s, const typename Tr<Real>::R2* __restrict__ trow, int rho,
-                                              int Q, Real (&aB)[kR], Real (&aC)[kR]) {
+                                              int Q, typename Tr<Real>::R2 (&acc)[kR]) {
   using R2 = typename Tr<Real>::R2;
-  Real pB[kR], pC[kR];
+  R2 pr[kR];
 #pragma unroll
-  for (int r = 0; r < kR; ++r) {
-    pB[r] = kTwoLevel ? (Real)0 : aB[r];
-    pC[r] = kTwoLevel ? (Real)0 : aC[r];
-  }
+  for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
   const int last = L - 1;
   int toff = rho;
   for (int q0 = 0; q0 < Q; q0 += kR) {
@@ -637,27 +643,23 @@ __device__ __forceinline__ void correlate_pre(const typename Tr<Real>::R2* __res
     int pos = base + q0 * s;
 #pragma unroll
     for (int m = 0; m < 2 * kR - 1; ++m) {
-      const R2 x = tile[min(pos, last)];
+      const R2 x = tile[kClamp ? min(pos, last) : pos];
       pos += s;
 #pragma unroll
       for (int qq = 0; qq < kR; ++qq) {
         const int r = m - qq;
         if (r >= 0 && r < kR) {
-          pB[r] = fma(tq[qq].x, x.x, pB[r]);
-          pC[r] = fma(tq[qq].y, x.y, pC[r]);
+          fma_pair(tq[qq], x, pr[r]);
         }
       }
     }
   }
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    if (kTwoLevel) {
-      aB[r] += pB[r];
-      aC[r] += pC[r];
-    } else {
-      aB[r] = pB[r];
-      aC[r] = pC[r];
-    }
+    if (kTwoLevel)
+      add_pair(acc[r], pr[r]);
+    else
+      acc[r] = pr[r];
   }
 }
 
@@ -667,13 +669,13 @@ __device__ __forceinline__ void correlate_pre(const typename Tr<Real>::R2* __res
 __constant__ int kLaneOf[2 * kR] = {0, 1, 2, 4, 5, 8, 9, 10, 12, 16, 17, 18, 20, 21, 24, 25, 26, 28};
 
 template <typename Real>
-__device__ __forceinline__ Real warp_reduce_scatter18(const Real (&aB)[kR], const Real (&aC)[kR]) {
+__device__ __forceinline__ Real warp_reduce_scatter18(const typename Tr<Real>::R2 (&acc)[kR]) {
   const int lane = threadIdx.x & 31;
   Real v[18];
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    v[r] = aB[r];
-    v[kR + r] = aC[r];
+    v[r] = acc[r].x;
+    v[kR + r] = acc[r].y;
   }
   // level xor 16: keep 9 of 18
   {
@@ -892,18 +894,22 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     const Real os = dtab_os[d];
     const Real inv_w = (Real)1 / (Real)w;
     const long long locb = (long long)upos * n;
-    Real aB[kR], aC[kR];
+    R2 acc[kR];
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      aB[r] = (Real)0;
-      aC[r] = (Real)0;
-    }
+    for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
     if (s >= kSplitMinSkip) {
       // lanes split the offset rho inside a skip block; one task = kR starts
       const int jb = jlo + sub * kR;
-      for (int rho = lane; rho < s; rho += 32)
-        correlate_pre<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
-      const Real mine = warp_reduce_scatter18<Real>(aB, aC);
+      // every load of the task inside the tile: no clamping needed
+      const int Qr = (Q + kR - 1) / kR * kR;
+      if ((jb + Qr + kR - 1) * s - k0 <= L) {
+        for (int rho = lane; rho < s; rho += 32)
+          correlate_pre<Real, kTwoLevel, false>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+      } else {
+        for (int rho = lane; rho < s; rho += 32)
+          correlate_pre<Real, kTwoLevel, true>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+      }
+      const Real mine = warp_reduce_scatter18<Real>(acc);
       // lane kLaneOf[r] holds B_r, lane kLaneOf[kR + r] holds C_r
       int r = -1;
 #pragma unroll
@@ -924,17 +930,17 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       if (jb < jhi) {
         const int Qr = (Q + kR - 1) / kR * kR;
         if (kAllStarts && s == 1 && jb + kR <= jhi) {
-          correlate_s1<Real, kTwoLevel>(tile, jb - k0, trow, Qr, aB, aC);
+          correlate_s1<Real, kTwoLevel>(tile, jb - k0, trow, Qr, acc);
         } else {
           for (int rho = 0; rho < s; ++rho)
-            correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, aB, aC);
+            correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const int j = jb + r;
           if (j < jhi) {
             const int k = j * s;
-            eval_start<Real>(best, pre, k, w, inv_w, os, aB[r], aC[r], a.depth_min, ebase, sentinel, locb + k);
+            eval_start<Real>(best, pre, k, w, inv_w, os, acc[r].x, acc[r].y, a.depth_min, ebase, sentinel, locb + k);
           }
         }
       }
