@@ -481,11 +481,9 @@ struct Chi2Args {
 
 // Mean depth of the window [k, k+w): -(sum v)/w  (calcAverageFromCumsum, GPUFun.py:366-375),
 // with 1/w computed once per duration.
-__device__ __forceinline__ double window_mean(const double* pre, int k, int w, double inv_w) {
-  return -(pre[k + w] - pre[k]) * inv_w;
-}
-__device__ __forceinline__ float window_mean(const float2* pre, int k, int w, float inv_w) {
-  float2 a = pre[k + w], b = pre[k];
+// From the two prefix values a = pre[k + w] and b = pre[k]:
+__device__ __forceinline__ double window_mean_of(double a, double b, double inv_w) { return -(a - b) * inv_w; }
+__device__ __forceinline__ float window_mean_of(float2 a, float2 b, float inv_w) {
   // two-diff of the high parts, then the low parts
   float s = a.x - b.x;
   float bb = s - a.x;
@@ -493,13 +491,15 @@ __device__ __forceinline__ float window_mean(const float2* pre, int k, int w, fl
   e += a.y - b.y;
   return -(s + e) * inv_w;
 }
+template <typename Pv, typename Real>
+__device__ __forceinline__ Real window_mean(const Pv* pre, int k, int w, Real inv_w) {
+  return window_mean_of(pre[k + w], pre[k], inv_w);
+}
 
 // Value of start k for duration d from its sums (B, C).
 template <typename Real>
-__device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::Pv* pre, int k, int w, Real inv_w,
-                                           Real os, Real B, Real C, double depth_min, double ebase,
-                                           double sentinel, long long loc) {
-  Real mean = window_mean(pre, k, w, inv_w);
+__device__ __forceinline__ void eval_mean(Best& best, Real mean, Real os, Real B, Real C, double depth_min,
+                                          double ebase, double sentinel, long long loc) {
   if ((double)mean > depth_min) {
     Real c = mean * os * (Real)2;
     Real delta = c * ((Real)2 * B + c * C);
@@ -507,6 +507,12 @@ __device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::
   } else {
     best_update(best, sentinel, loc);
   }
+}
+template <typename Real>
+__device__ __forceinline__ void eval_start(Best& best, const typename Tr<Real>::Pv* pre, int k, int w, Real inv_w,
+                                           Real os, Real B, Real C, double depth_min, double ebase,
+                                           double sentinel, long long loc) {
+  eval_mean<Real>(best, window_mean(pre, k, w, inv_w), os, B, C, depth_min, ebase, sentinel, loc);
 }
 
 // (b, c) += (t.x * x.x, t.y * x.y) for an accumulator pair (B, C): one
@@ -935,12 +941,23 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
           for (int rho = 0; rho < s; ++rho)
             correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
+        // the prefix values of the lane's kR starts, all loads in flight
+        // together (indices clamped to the last start of the tile; values of
+        // starts past it are discarded)
+        Pv p0[kR], pw[kR];
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+          const int k = min(jb + r, jhi - 1) * s;
+          p0[r] = pre[k];
+          pw[r] = pre[k + w];
+        }
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const int j = jb + r;
           if (j < jhi) {
             const int k = j * s;
-            eval_start<Real>(best, pre, k, w, inv_w, os, acc[r].x, acc[r].y, a.depth_min, ebase, sentinel, locb + k);
+            eval_mean<Real>(best, window_mean_of(pw[r], p0[r], inv_w), os, acc[r].x, acc[r].y, a.depth_min, ebase,
+                            sentinel, locb + k);
           }
         }
       }
