@@ -127,7 +127,10 @@ class gtls_batch(object):
     takes the keywords of ``gtls.power`` (applied to every curve) plus
     ``full_stats`` (default False: period, duration, depth, T0 and SDE only;
     True adds transit times and the SNRs) and ``keep_spectra`` (default
-    True: each result carries its periods, power and chi2)."""
+    True: each result carries its periods, power and chi2).  With
+    ``distributed=True`` under an initialised torch.distributed process group
+    (one process per GPU) every rank searches a work-balanced share of the
+    curves and all ranks return every curve's result."""
 
     def __init__(self, curves, verbose=False):
         self.curves = [tuple(c) + (None,) * (3 - len(c)) for c in curves]
@@ -145,9 +148,18 @@ class gtls_batch(object):
         device = opts.GPUDeviceID
         if opts.GPUDeviceIDs:
             device = opts.GPUDeviceIDs[0]
-        prepared = [prepare_curve(t, y, dy, opts, device=device) for (t, y, dy) in self.curves]
-        return search_prepared(prepared, opts, device=device, full_stats=full_stats, keep_spectra=keep_spectra,
-                               timing=timing)
+        def search_subset(indices):
+            prepared = [prepare_curve(*self.curves[i], opts, device=device) for i in indices]
+            return search_prepared(prepared, opts, device=device, full_stats=full_stats,
+                                   keep_spectra=keep_spectra, timing=timing)
+
+        if opts.distributed:
+            # each rank searches a share of the curves balanced by estimated
+            # work (samples x time span, which the period count follows)
+            from . import shard
+            costs = [len(c[0]) * float(np.ptp(np.asarray(c[0], dtype=np.float64))) for c in self.curves]
+            return shard.sharded_curves(costs, search_subset)
+        return search_subset(list(range(len(self.curves))))
 
 
 def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None):

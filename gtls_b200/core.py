@@ -117,7 +117,7 @@ def _candidates(power_dev, mask_dev, periods_dev, torch):
 
 def search_multi_periods(periods, t, y, dy, transit_depth_min, lc_arr, lc_cache_overview, T0_fit_margin,
                          oversampling_factor, verbose=False, GPUDeviceID=0, fast=False, precision="fp64",
-                         batch_periods=None):
+                         batch_periods=None, distributed=False):
     """GPU counterpart of core.search_multi_periods (core.py:568-999).
 
     Returns the reference's 19 values (periods, period, rawDuration,
@@ -131,27 +131,50 @@ def search_multi_periods(periods, t, y, dy, transit_depth_min, lc_arr, lc_cache_
     cur = CurveOnDevice(t, y, dy, lc_arr, lc_cache_overview, device=GPUDeviceID)
     periods_dev = _h2d(torch, periods, cur.dev)
     return run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_margin, oversampling_factor,
-                      fast=fast, precision=precision, batch_periods=batch_periods)
+                      fast=fast, precision=precision, batch_periods=batch_periods, distributed=distributed)
 
 
 def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_margin, oversampling_factor,
-               fast=False, precision="fp64", batch_periods=None, timing=None):
+               fast=False, precision="fp64", batch_periods=None, timing=None, distributed=False, group=None):
     """The search on a curve already resident on the device (see search_multi_periods).
 
     ``periods``: sorted host array, ``periods_dev`` the same on the device.
     ``timing``: optional ``_lib.Timing`` receiving the main pass's stage times.
+    ``distributed``: shard the main pass over the ranks of the initialised
+    process group ``group`` (batch-aligned period ranges, chi2 all-gathered);
+    every rank then finishes the search and returns the same result.
     """
     import torch
+    from . import shard
     device = cur.device
     skip = skip_point_of(T0_fit_margin)
+    rank, world = shard.world_info(group) if distributed else (0, 1)
     if batch_periods is None:
         free = torch.cuda.mem_get_info(device)[0]
         batch_periods = reference_batch_size(len(periods), cur.n, cur.maxd, len(cur.widths), free)
+        if world > 1:
+            # every rank must use rank 0's batch size (the free memory differs)
+            import torch.distributed as dist
+            obj = [batch_periods]
+            dist.broadcast_object_list(obj, src=0, group=group)
+            batch_periods = obj[0]
     S = int(batch_periods)
     dev = cur.dev
 
-    chi2_dev, _ = cur.search(periods_dev, transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision,
-                             timing=timing)
+    if world > 1:
+        import torch.distributed as dist
+        nccl = dist.get_backend(group) == "nccl"
+
+        def main_pass(p0, p1):
+            c, _ = cur.search(periods_dev[p0:p1], transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision,
+                              timing=timing)
+            return c if nccl else c.cpu()
+
+        chi2_dev = shard.sharded_period_pass(len(periods), S, main_pass, group=group,
+                                             device=dev if nccl else None).to(dev)
+    else:
+        chi2_dev, _ = cur.search(periods_dev, transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision,
+                                 timing=timing)
     raw_chi2 = _d2h(chi2_dev)
     median = np.median(raw_chi2)
     mask = raw_chi2 > (100 * median)

@@ -3,12 +3,16 @@
 Same constructor, same ``power()`` keywords (constants.VALID_PARAMETERS) and
 the same return: a ``gtlsResult`` or, with ``fast=True``, ``(periods, power)``.
 The search runs on one GPU (``GPUDeviceID``); ``GPUDeviceIDs`` with more than
-one entry is accepted and runs on the first device (multi-GPU sharding of a
-single light curve is not part of this implementation).
+one entry is accepted and runs on the first device: the reference's own
+multi-GPU mode (worker processes per GPU) is replaced by ``distributed``
+below, with one process per GPU started by torchrun.
 Extra keywords: ``precision`` ("fp64" plain FP64 search, default; "fp32" FP32
-chi2 with compensated prefix sums and FP64 re-search of the candidates) and
+chi2 with compensated prefix sums and FP64 re-search of the candidates),
 ``batch_periods`` (periods per duration-union batch; default: the reference's
-free-memory formula, core.py:620-628).
+free-memory formula, core.py:620-628) and ``distributed`` (shard the main pass
+over the ranks of the initialised torch.distributed process group, one
+process per GPU: batch-aligned period ranges, chi2 all-gathered; every rank
+returns the same result).
 """
 import warnings
 
@@ -64,7 +68,8 @@ class gtls(object):
             periods=periods, t=self.t, y=self.y, dy=self.dy, transit_depth_min=self.transit_depth_min,
             lc_arr=self.lc_arr, lc_cache_overview=self.lc_cache_overview, T0_fit_margin=self.T0_fit_margin,
             oversampling_factor=self.oversampling_factor, verbose=self.verbose, GPUDeviceID=self.GPUDeviceID,
-            fast=self.fast, precision=self.precision, batch_periods=self.batch_periods)
+            fast=self.fast, precision=self.precision, batch_periods=self.batch_periods,
+            distributed=self.distributed)
         if self.fast:
             return out
         (self.periods, self.period, self.rawDuration, durationPoints, self.duration, self.Depth, self.bestT0,

@@ -113,6 +113,9 @@ def validate_args(self, kwargs):
     if self.precision not in ("fp64", "fp32"):
         raise ValueError('precision must be "fp64" or "fp32"')
     self.batch_periods = kwargs.get("batch_periods", None)
+    # distributed: shard the search over the ranks of the initialised
+    # torch.distributed process group (one process per GPU)
+    self.distributed = bool(kwargs.get("distributed", False))
 
     if "b" in kwargs:
         self.b = kwargs.get("b")
