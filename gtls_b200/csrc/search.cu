@@ -1185,7 +1185,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     const size_t table = (size_t)D * (sizeof(Real) + 2 * sizeof(int)) + 16;
     long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd - kTilePad) / 256 * 256;
     if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
-    tile = std::min<long long>(tile, 8192);
+    tile = std::min<long long>(tile, sizeof(Real) == 4 ? 16384 : 8192);   // measured best caps
     if (tile > n) tile = (n + 255) / 256 * 256;
     C.t = h.t;
     C.y = h.y;
