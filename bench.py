@@ -326,6 +326,8 @@ def bench_batch(args):
     validate_args(opts, dict(precision=args.precision, use_threads=1, GPUDeviceID=device))
     prepared = [batch.prepare_curve(t, y, None, opts, device=device) for (t, y) in curves]
     cs = batch.CurveSetOnDevice(prepared, device=device)
+    from gtls_b200 import tune
+    tuning = tune.tune_curve_set(cs, args.precision)   # launch shapes chosen on this data (untimed)
     work = float(sum(len(p["t"]) * len(p["periods"]) for p in prepared))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cs.dev)
     for _ in range(args.warmup):
@@ -380,7 +382,7 @@ def bench_batch(args):
                    "work_fraction_of_4096_set": work / total_work,
                    "full_set_seconds_estimate": ms * 1e-3 * total_work / work,
                    "l2": "flushed (256 MB write) before every timed step; per-chunk scratch > L2",
-                   "precision": args.precision},
+                   "precision": args.precision, "tuning": tuning},
         "e2e": {"value": len(idx) * 1000.0 / e2e_ms, "unit": "light curves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),

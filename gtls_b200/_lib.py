@@ -87,6 +87,16 @@ class SearchDesc(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    """Mirror of ``gtls_tuning``."""
+    _fields_ = [
+        ("tile_cap_fp32", ctypes.c_int32),
+        ("tile_cap_fp64", ctypes.c_int32),
+        ("bucket_shift", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class BatchDesc(ctypes.Structure):
     """Mirror of ``gtls_batch_desc``."""
     _fields_ = [
@@ -124,6 +134,8 @@ EXPORTS = {
     "gtls_abi_version": ([], ctypes.c_int),
     "gtls_launch_count": ([ctypes.c_void_p], ctypes.c_int64),
     "gtls_set_chunk_budget": ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
+    "gtls_set_tuning": ([ctypes.c_void_p, ctypes.POINTER(Tuning)], ctypes.c_int),
+    "gtls_get_tuning": ([ctypes.c_void_p, ctypes.POINTER(Tuning)], ctypes.c_int),
     "gtls_period_grid": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
                           ctypes.c_double, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p],
                          ctypes.c_int),
@@ -236,6 +248,22 @@ def set_chunk_budget(nbytes, device=0):
     """Per-chunk scratch budget of the searches on ``device`` (bytes)."""
     ctx = context(device)
     _check(load().gtls_set_chunk_budget(ctx, int(nbytes)), ctx, "gtls_set_chunk_budget")
+
+
+def set_tuning(tile_cap_fp32=0, tile_cap_fp64=0, bucket_shift=0, device=0):
+    """Launch-shape parameters of the searches on ``device`` (0 = default);
+    results do not depend on them."""
+    ctx = context(device)
+    t = Tuning(int(tile_cap_fp32), int(tile_cap_fp64), int(bucket_shift), 0)
+    _check(load().gtls_set_tuning(ctx, ctypes.byref(t)), ctx, "gtls_set_tuning")
+
+
+def get_tuning(device=0):
+    """The current ``Tuning`` of ``device`` as a dict."""
+    ctx = context(device)
+    t = Tuning()
+    _check(load().gtls_get_tuning(ctx, ctypes.byref(t)), ctx, "gtls_get_tuning")
+    return dict(tile_cap_fp32=t.tile_cap_fp32, tile_cap_fp64=t.tile_cap_fp64, bucket_shift=t.bucket_shift)
 
 
 def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precision, device=0,

@@ -127,7 +127,9 @@ class gtls_batch(object):
     takes the keywords of ``gtls.power`` (applied to every curve) plus
     ``full_stats`` (default False: period, duration, depth, T0 and SDE only;
     True adds transit times and the SNRs) and ``keep_spectra`` (default
-    True: each result carries its periods, power and chi2).  With
+    True: each result carries its periods, power and chi2) and ``autotune``
+    (default True: launch shapes timed and chosen on the data, see
+    ``gtls_b200.tune``; results do not depend on them).  With
     ``distributed=True`` under an initialised torch.distributed process group
     (one process per GPU) every rank searches a work-balanced share of the
     curves and all ranks return every curve's result."""
@@ -140,6 +142,7 @@ class gtls_batch(object):
 
     def power(self, **kwargs):
         full_stats = bool(kwargs.pop("full_stats", False))
+        autotune = bool(kwargs.pop("autotune", True))
         keep_spectra = bool(kwargs.pop("keep_spectra", True))
         timing = kwargs.pop("timing", None)
         kwargs.setdefault("precision", "fp32")
@@ -151,7 +154,7 @@ class gtls_batch(object):
         def search_subset(indices):
             prepared = [prepare_curve(*self.curves[i], opts, device=device) for i in indices]
             return search_prepared(prepared, opts, device=device, full_stats=full_stats,
-                                   keep_spectra=keep_spectra, timing=timing)
+                                   keep_spectra=keep_spectra, timing=timing, autotune=autotune)
 
         if opts.distributed:
             # each rank searches a share of the curves balanced by estimated
@@ -162,13 +165,18 @@ class gtls_batch(object):
         return search_subset(list(range(len(self.curves))))
 
 
-def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None):
+def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None, autotune=False):
     """The batched search of curves already prepared by ``prepare_curve``.
 
     Returns one ``types.SimpleNamespace`` per curve with period, duration,
     depth, T0, SDE, SDE_raw, period_index, width, rawDuration and (with
-    ``keep_spectra``) periods, power and chi2 as masked arrays."""
+    ``keep_spectra``) periods, power and chi2 as masked arrays.  With
+    ``autotune`` the launch shapes are first tuned on the set's largest
+    curve (``tune.tune_curve_set``; cached per shape, results unchanged)."""
     cs = CurveSetOnDevice(prepared, device=device)
+    if autotune:
+        from . import tune
+        tune.tune_curve_set(cs, opts.precision)
     return search_on_device(cs, opts, full_stats=full_stats, keep_spectra=keep_spectra, timing=timing)
 
 

@@ -228,6 +228,28 @@ int gtls_abi_version(void) { return GTLS_ABI_VERSION; }
 
 int64_t gtls_launch_count(const gtls_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int gtls_set_tuning(gtls_ctx* ctx, const gtls_tuning* t) {
+  if (!ctx) return GTLS_E_INVALID;
+  if (!t) return fail(ctx, GTLS_E_INVALID, "null tuning");
+  auto cap_ok = [](int c) { return c == 0 || (c >= 256 && c <= 65536 && c % 256 == 0); };
+  if (!cap_ok(t->tile_cap_fp32) || !cap_ok(t->tile_cap_fp64))
+    return fail(ctx, GTLS_E_INVALID, "tile caps must be 0 or multiples of 256 in [256, 65536]");
+  if (t->bucket_shift < -3 || t->bucket_shift > 0) return fail(ctx, GTLS_E_INVALID, "bucket_shift must be in [-3, 0]");
+  ctx->tile_cap_fp32 = t->tile_cap_fp32 ? t->tile_cap_fp32 : 16384;
+  ctx->tile_cap_fp64 = t->tile_cap_fp64 ? t->tile_cap_fp64 : 8192;
+  ctx->bucket_shift = t->bucket_shift;
+  return GTLS_OK;
+}
+
+int gtls_get_tuning(const gtls_ctx* ctx, gtls_tuning* t) {
+  if (!ctx || !t) return GTLS_E_INVALID;
+  t->tile_cap_fp32 = ctx->tile_cap_fp32;
+  t->tile_cap_fp64 = ctx->tile_cap_fp64;
+  t->bucket_shift = ctx->bucket_shift;
+  t->reserved = 0;
+  return GTLS_OK;
+}
+
 int gtls_set_chunk_budget(gtls_ctx* ctx, uint64_t bytes) {
   if (!ctx) return GTLS_E_INVALID;
   if (bytes < ((uint64_t)1 << 20)) return fail(ctx, GTLS_E_INVALID, "chunk budget must be >= 1 MiB");

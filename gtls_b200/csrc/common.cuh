@@ -17,6 +17,9 @@ struct gtls_ctx {
   int* status = nullptr;       // device status word(s) written by kernels
   long long launches = 0;      // kernels launched through this context
   size_t chunk_budget = (size_t)8 << 30;   // per-chunk scratch of a search, bytes
+  int tile_cap_fp32 = 16384;   // launch-shape tuning (gtls_set_tuning); results do not depend on it
+  int tile_cap_fp64 = 8192;
+  int bucket_shift = 0;
 };
 
 namespace gtls {

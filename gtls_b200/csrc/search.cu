@@ -590,8 +590,9 @@ __device__ __forceinline__ void correlate(const typename Tr<Real>::R2* __restric
 // clamping (the reads stay inside the tile and its zeroed pad), whole blocks
 // of kR template entries (entries past Q are zero), consecutive records and
 // template entries addressed with constant offsets from block pointers.  The
-// FP32 form adds each block of kR products to the running sums separately
-// (two-level summation).
+// sums are formed in exactly the order of correlate() with skip 1 (entries
+// past Q add exact zeros), so a start's value does not depend on which of
+// the two paths the tile boundaries send it through.
 template <typename Real, bool kTwoLevel>
 __device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __restrict__ tile, int base,
                                              const typename Tr<Real>::R2* __restrict__ trow, int Qr,
@@ -601,10 +602,10 @@ __device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __rest
   const R2* xp = tile + base;
 #pragma unroll
   for (int i = 0; i < kR - 1; ++i) xs[i] = xp[i];
-  for (int q0 = 0; q0 < Qr; q0 += kR) {
-    R2 pr[kR];
+  R2 pr[kR];
 #pragma unroll
-    for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
+  for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
+  for (int q0 = 0; q0 < Qr; q0 += kR) {
     const R2* xb = xp + q0 + kR - 1;
     const R2* tb = trow + q0;
 #pragma unroll
@@ -612,18 +613,15 @@ __device__ __forceinline__ void correlate_s1(const typename Tr<Real>::R2* __rest
       xs[(qq + kR - 1) % kR] = xb[qq];
       const R2 tq = tb[qq];
 #pragma unroll
-      for (int r = 0; r < kR; ++r) {
-        const R2 x = xs[(qq + r) % kR];
-        fma_pair(tq, x, pr[r]);
-      }
+      for (int r = 0; r < kR; ++r) fma_pair(tq, xs[(qq + r) % kR], pr[r]);
     }
+  }
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      if (kTwoLevel)
-        add_pair(acc[r], pr[r]);
-      else
-        acc[r] = pr[r];
-    }
+  for (int r = 0; r < kR; ++r) {
+    if (kTwoLevel)
+      add_pair(acc[r], pr[r]);
+    else
+      acc[r] = pr[r];
   }
 }
 
@@ -1121,10 +1119,11 @@ __global__ void template_rows_kernel(const CurveDev<Real>* __restrict__ cds, con
 }
 
 // ------------------------------------------------------------------ host
-static int nb_log2_for(int n) {
+static int nb_log2_for(int n, int shift) {
   int k = 1;
-  while ((1 << k) < n && k < 15) ++k;  // at most 32768 buckets (128 KB of counters)
-  return k;
+  while ((1 << k) < n) ++k;
+  k = std::min(15, k + shift);   // at most 32768 buckets (128 KB of counters)
+  return std::max(1, k);
 }
 
 // One light curve of a search, as the host sees it.
@@ -1185,7 +1184,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     const size_t table = (size_t)D * (sizeof(Real) + 2 * sizeof(int)) + 16;
     long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd - kTilePad) / 256 * 256;
     if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
-    tile = std::min<long long>(tile, sizeof(Real) == 4 ? 16384 : 8192);   // measured best caps
+    tile = std::min<long long>(tile, sizeof(Real) == 4 ? ctx->tile_cap_fp32 : ctx->tile_cap_fp64);
     if (tile > n) tile = (n + 255) / 256 * 256;
     C.t = h.t;
     C.y = h.y;
@@ -1207,7 +1206,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     C.nbatch = (int)((h.np + h.batch - 1) / h.batch);
     C.tile = (int)tile;
     C.ntiles = (int)((n + tile - 1) / tile);
-    C.nb_log2 = nb_log2_for(n);
+    C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
     C.span = h.span;
     p_off[c + 1] = p_off[c] + h.np;
     b_off[c + 1] = b_off[c] + C.nbatch;

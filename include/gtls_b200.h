@@ -68,6 +68,23 @@ int64_t gtls_launch_count(const gtls_ctx* ctx);
  * bytes must be >= 1 MiB. */
 int gtls_set_chunk_budget(gtls_ctx* ctx, uint64_t bytes);
 
+/* Launch-shape parameters of the searches on a context (no counterpart in
+ * the reference).  None changes a result: chi2 values and argmin locations
+ * are the same for every setting; only the time differs, so a caller (or
+ * gtls_b200.tune) may time a few settings on its own data and keep the
+ * fastest.  A zero field means the default. */
+typedef struct gtls_tuning {
+  int32_t tile_cap_fp32;      /* max starts per chi2 tile (CTA), FP32 form: a multiple of 256 in
+                                 [256, 65536], or 0 = 16384.  The shared-memory size caps it too. */
+  int32_t tile_cap_fp64;      /* the same for the FP64 form, 0 = 8192                        */
+  int32_t bucket_shift;       /* phase buckets of the fold ordering = 2^min(15, ceil(log2 N) + shift),
+                                 shift in [-3, 0] (0 = default)                               */
+  int32_t reserved;           /* 0                                                            */
+} gtls_tuning;
+
+int gtls_set_tuning(gtls_ctx* ctx, const gtls_tuning* tuning);
+int gtls_get_tuning(const gtls_ctx* ctx, gtls_tuning* tuning);
+
 /*
  * Ofir-optimal period grid, evaluated on the device.
  * Replaces the per-point part of grid.period_grid (grid.py:126-137):
