@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--curves", type=int, default=32,
                     help="cfg4: curves per step (every 4096/curves-th curve of the 4,096-curve set)")
     ap.add_argument("--no-per-curve", action="store_true", help="cfg4: skip the per-curve FP64 comparison")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="cfg4: only the agreement of the batched FP32 search with the plain FP64 per-curve "
+                         "search over the sample (one pass each), no timing steps")
     ap.add_argument("--chunk-mb", type=int, default=0,
                     help="per-chunk scratch budget of the searches in MiB (default: the library's 8 GiB)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -277,6 +280,57 @@ def cpu_reference_work(t, y, dy, budget_s, seed=0):
     return r["seconds_per_curve"] / (len(t) * len(periods)), r
 
 
+def cfg4_accuracy(args, curves, idx, specs, device):
+    """Agreement of the batched FP32-compensated search with the plain FP64
+    per-curve search on the same curves: best period index, best duration
+    (width), SDE, depth and T0."""
+    import types
+    import torch
+    from gtls_b200 import core, gtls
+    from gtls_b200.batch import gtls_batch, prepare_curve
+    from gtls_b200.validate import validate_args
+    # the reference sizes its duration-union batches from the free GPU memory
+    # (core.py:620-628), which differs between one batched call and many
+    # single-curve calls; both sides get the sizes of the same free-memory figure
+    free0 = torch.cuda.mem_get_info(device)[0]
+    opts = types.SimpleNamespace()
+    validate_args(opts, dict(use_threads=1, GPUDeviceID=device))
+    S = []
+    for (t, y) in curves:
+        p = prepare_curve(t, y, None, opts, device=device)
+        S.append(core.reference_batch_size(len(p["periods"]), len(p["t"]), p["maxd"], len(p["widths"]), free0))
+    a = time.perf_counter()
+    rb = gtls_batch(curves).power(precision=args.precision, use_threads=1, GPUDeviceID=device, keep_spectra=False,
+                                  batch_periods=np.array(S))
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - a
+    a = time.perf_counter()
+    r64 = [gtls(t, y, verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device, batch_periods=int(s))
+           for (t, y), s in zip(curves, S)]
+    torch.cuda.synchronize()
+    t_64 = time.perf_counter() - a
+    same_p = np.array([x.period == y.period for x, y in zip(rb, r64)])
+    same_w = np.array([x.width == y.durationPoints for x, y in zip(rb, r64)])
+    rel = lambda u, v: abs(u - v) / max(abs(v), 1e-300)
+    sde = np.array([rel(x.SDE, y.SDE) for x, y in zip(rb, r64)])
+    dep = np.array([rel(x.depth, y.depth) for x, y in zip(rb, r64)])
+    t0 = np.array([abs(x.T0 - y.T0) for x, y in zip(rb, r64)])
+    line = {"metric": "agreement of the batched FP32-compensated search with the plain FP64 per-curve search",
+            "config": {"workload": "cfg4: every %d-th of the 4,096 seeded synthetic curves" % (4096 // len(idx)),
+                       "curves": len(idx), "precision": args.precision},
+            "best_period_index_agreement": float(same_p.mean()), "disagreeing_curves": [int(i) for i in idx[~same_p]],
+            "best_duration_agreement": float(same_w.mean()),
+            "SDE_max_rel_diff": float(sde.max()), "SDE_median_rel_diff": float(np.median(sde)),
+            "depth_max_rel_diff_same_index": float(dep[same_p].max()) if same_p.any() else None,
+            "T0_max_abs_diff_days_same_index": float(t0[same_p].max()) if same_p.any() else None,
+            "seconds": {"batched": t_batch, "per_curve_fp64": t_64},
+            "recovered_1pct": int(sum(abs(r.period - specs["period"][i]) < 0.01 * specs["period"][i]
+                                      for r, i in zip(rb, idx) if specs["has_transit"][i])),
+            "with_transit": int(sum(bool(specs["has_transit"][i]) for i in idx))}
+    print(json.dumps(line))
+    return 0
+
+
 def bench_batch(args):
     """cfg4: batched search of a fixed sample of the 4,096-curve set per step."""
     import types
@@ -322,6 +376,8 @@ def bench_batch(args):
         return 0
 
     device = torch.cuda.current_device()
+    if args.accuracy:
+        return cfg4_accuracy(args, curves, idx, specs, device)
     opts = types.SimpleNamespace()
     validate_args(opts, dict(precision=args.precision, use_threads=1, GPUDeviceID=device))
     prepared = [batch.prepare_curve(t, y, None, opts, device=device) for (t, y) in curves]

@@ -151,9 +151,17 @@ class gtls_batch(object):
         device = opts.GPUDeviceID
         if opts.GPUDeviceIDs:
             device = opts.GPUDeviceIDs[0]
+        per_curve_batch = opts.batch_periods is not None and np.ndim(opts.batch_periods) > 0
+        if per_curve_batch and len(opts.batch_periods) != len(self.curves):
+            raise ValueError("batch_periods must be one value or one per curve")
+
         def search_subset(indices):
-            prepared = [prepare_curve(*self.curves[i], opts, device=device) for i in indices]
-            return search_prepared(prepared, opts, device=device, full_stats=full_stats,
+            sub = opts
+            if per_curve_batch:
+                sub = types.SimpleNamespace(**vars(opts))
+                sub.batch_periods = np.asarray(opts.batch_periods)[list(indices)]
+            prepared = [prepare_curve(*self.curves[i], sub, device=device) for i in indices]
+            return search_prepared(prepared, sub, device=device, full_stats=full_stats,
                                    keep_spectra=keep_spectra, timing=timing, autotune=autotune)
 
         if opts.distributed:
