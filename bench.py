@@ -644,6 +644,8 @@ def main():
     free = torch.cuda.mem_get_info(device)[0]
     batch = core.reference_batch_size(len(periods), cur.n, cur.maxd, len(cur.widths), free)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cur.dev)  # > 126 MB L2
+    from gtls_b200 import tune
+    tuning = tune.tune_curve(cur, periods, args.precision)   # launch shapes chosen on this data (untimed)
 
     def one_step(timing=None):
         return core.run_search(cur, periods, periods_dev, t, y, dy, 1e-5, 0.125, kw["oversampling_factor"],
@@ -733,7 +735,7 @@ def main():
         "config": {"workload": desc, "periods": len(periods), "durations": len(cur.widths), "samples": n,
                    "batch_periods": batch, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed (256 MB write) before every timed step; per-period scratch > L2",
-                   "precision": args.precision},
+                   "precision": args.precision, "tuning": tuning},
         "e2e": {"value": world * 1000.0 / e2e_ms_step, "unit": "light curves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms_step},
         "gpu_launches": int(launches // args.steps),

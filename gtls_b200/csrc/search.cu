@@ -18,8 +18,8 @@
 // which is what these kernels evaluate.  B and C are sliding correlations of
 // the template with the folded (u, w) records; the work is FMA-bound and runs
 // on the FP64 or FP32 pipes (nothing here is a dense contraction, so no tensor
-// cores).  The mean depth comes from prefix sums of v (FP64, or compensated
-// float-float in the FP32 form).  Only starts k that are multiples of
+// cores).  The mean depth comes from prefix sums of v (FP64; stored as
+// float-float pairs in the FP32 form).  Only starts k that are multiples of
 // skip(d) = w / skip_point (for w > skip_point) are evaluated in the main pass
 // (GPUFun.py:402,409); every other (d,k) carries the value n
 // (GPUFun.py:407,437), which takes part in the minimum like any value.
@@ -28,8 +28,9 @@
 //   curve_setup_kernel   (v, w) records per original sample and E.
 //   prepare_kernel       one CTA per period: FP64 fold (GPUFun.py:30-41),
 //                        stable bucket ranking of the phases (cupy argsort),
-//                        gather into the padded sorted record array
-//                        (patchData GPUFun.py:110-129) and the prefix of v.
+//                        each ranked sample written straight to its place in
+//                        the padded sorted record array (patchData
+//                        GPUFun.py:110-129), then the prefix of v.
 //   chi2_kernel          one CTA per (period, tile of starts): the tile of
 //                        records is staged in shared memory, warps pull
 //                        (duration, start-group) tasks from a CTA-local queue,
@@ -253,13 +254,14 @@ __device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __rest
   return a.y < b.y;
 }
 
-// Rank of every entry of bucket slots [s, e) among the bucket (ord[s + rank] =
-// original index), by a whole warp: each lane ranks one entry of a group of
+// Rank of every entry of bucket slots [s, e) among the bucket (emit(s + rank,
+// original index)), by a whole warp: each lane ranks one entry of a group of
 // 32 against the bucket, streamed 32 entries at a time and broadcast by
 // shuffles.  Used for large buckets, whose O(k^2) comparisons would
 // otherwise fall on single threads.
-__device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot, int* __restrict__ ord, int s, int e,
-                                                 const double* __restrict__ t, double P) {
+template <typename Emit>
+__device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot, int s, int e,
+                                                 const double* __restrict__ t, double P, Emit emit) {
   const int lane = threadIdx.x & 31;
   for (int j0 = s; j0 < e; j0 += 32) {
     const int j = j0 + lane;
@@ -275,14 +277,14 @@ __device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot,
         if (o.y != mine.y && slot_less(o, mine, t, P)) ++r;
       }
     }
-    if (j < e) ord[s + r] = (int)mine.y;
+    if (j < e) emit(s + r, (int)mine.y);
   }
 }
 
 template <typename Real>
 __global__ void __launch_bounds__(kPrepThreads)
 prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
-               uint2* __restrict__ scr_slot, int* __restrict__ scr_ord, typename Tr<Real>::R2* __restrict__ rec,
+               uint2* __restrict__ scr_slot, typename Tr<Real>::R2* __restrict__ rec,
                typename Tr<Real>::Pv* __restrict__ pv) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
@@ -306,7 +308,6 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   const int M = C.M;
   const int Mrec = C.Mrec;
   uint2* slot = scr_slot + R.slot_off + (size_t)local * n;
-  int* ord = scr_ord + R.slot_off + (size_t)local * n;
   R2* out = rec + R.rec_off + (size_t)local * Mrec;
   Pv* pre = pv + R.pv_off + (size_t)local * (M + 1);
   double* pre_d = reinterpret_cast<double*>(pre);   // FP64 view during the scan (Pv is 8 bytes)
@@ -354,7 +355,24 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
     }
   }
   __syncthreads();
-  // (3) ranking within buckets: ord[start + rank] = original index.
+  // (3) ranking within buckets.  The entry of final sorted position p and
+  //     original sample i is emitted at once: its record (u, w) at p, v at
+  //     pre[p + 1] for the scan, and the same at n + p when p < maxd (the
+  //     wrap of patchData, GPUFun.py:110-129); i is clamped so that a
+  //     malformed input can never address outside the curve.
+  auto emit = [&](int p, int i) {
+    i = min(max(i, 0), n - 1);
+    const double2 g = vw[i];
+    R2 o;
+    o.x = (Real)(g.x * g.y);
+    o.y = (Real)g.y;
+    out[p] = o;
+    pre_d[p + 1] = g.x;
+    if (p < maxd) {
+      out[p + n] = o;
+      pre_d[p + n + 1] = g.x;
+    }
+  };
   //     (a) buckets of more than kSmallBucket entries (clustered phases, as
   //         when the period is close to a multiple of a regular cadence) are
   //         listed, from the shared-memory counts alone;
@@ -371,10 +389,12 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   if (warp_ranked)
     for (int q = (int)(threadIdx.x >> 5); q < nbig; q += (int)(blockDim.x >> 5)) {
       const int b = big[q];
-      rank_bucket_warp(slot, ord, b == 0 ? 0 : hist[b - 1], hist[b], t, P);
+      rank_bucket_warp(slot, b == 0 ? 0 : hist[b - 1], hist[b], t, P, emit);
     }
   //     (c) every other entry is ranked by its own thread: coalesced over the
-  //         slots, its bucket found by binary search of the bucket ends.
+  //         slots, its bucket found by binary search of the bucket ends (the
+  //         emitted positions are then close to the slot index, so the
+  //         record writes stay nearly coalesced).
   for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
@@ -390,40 +410,13 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
         const int e = hist[lo];
         const uint2 sj = slot[j];
         if (e - s == 1) {
-          ord[j] = (int)sj.y;
+          emit(j, (int)sj.y);
         } else if (e - s <= kSmallBucket || !warp_ranked) {
           int r = 0;
           for (int m = s; m < e; ++m)
             if (m != j) r += slot_less(slot[m], sj, t, P);
-          ord[s + r] = (int)sj.y;
+          emit(s + r, (int)sj.y);
         }
-      }
-    }
-  }
-  __syncthreads();
-  // (4) gather (u, w) into the padded sorted order (patchData) and keep v in
-  //     pre[r + 1] for the scan; indices are clamped so that a malformed
-  //     input can never address outside the curve
-  for (int r0 = threadIdx.x; r0 < M; r0 += stride) {
-    int ii[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int r = r0 + u * blockDim.x;
-      ii[u] = r < M ? ord[r < n ? r : r - n] : 0;
-      ii[u] = min(max(ii[u], 0), n - 1);
-    }
-    double2 g[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) g[u] = vw[ii[u]];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int r = r0 + u * blockDim.x;
-      if (r < M) {
-        R2 o;
-        o.x = (Real)(g[u].x * g[u].y);
-        o.y = (Real)g[u].y;
-        out[r] = o;
-        pre_d[r + 1] = g[u].x;
       }
     }
   }
@@ -1251,7 +1244,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     };
     for (int c = 0; c < n_curves; ++c) {
       const CurveDev<Real>& C = cd[c];
-      const size_t per = (size_t)C.n * 12 + (size_t)C.Mrec * sizeof(R2) + (size_t)(C.M + 1) * sizeof(Pv) +
+      const size_t per = (size_t)C.n * 8 + (size_t)C.Mrec * sizeof(R2) + (size_t)(C.M + 1) * sizeof(Pv) +
                          (size_t)C.ntiles * 16;
       long long p = 0;
       while (p < C.np) {
@@ -1297,7 +1290,6 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   carve_size<Run>(total, std::max(1, nruns_total));
   carve_size<long long>(total, 3 * (size_t)(n_curves + 1));
   carve_size<uint2>(total, max_slot);
-  carve_size<int>(total, max_slot);
   carve_size<R2>(total, max_rec);
   carve_size<Pv>(total, max_pv);
   carve_size<double>(total, max_part);
@@ -1332,7 +1324,6 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   Run* d_runs = cv.take<Run>(std::max(1, nruns_total));
   long long* d_offs = cv.take<long long>(3 * (size_t)(n_curves + 1));
   uint2* scr_slot = cv.take<uint2>(max_slot);
-  int* scr_ord = cv.take<int>(max_slot);
   R2* rec = cv.take<R2>(max_rec);
   Pv* pv = cv.take<Pv>(max_pv);
   double* part_v = cv.take<double>(max_part);
@@ -1398,8 +1389,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
       for (auto& e : e3) GTLS_TRY_CUDA(ctx, cudaEventCreate(&e));
       GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[0], st));
     }
-    prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, scr_ord,
-                                                                          rec, pv);
+    prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
     ca.nruns = nr;
     if (all)

@@ -77,3 +77,16 @@ def tune_curve_set(cs, precision, n_sample=600, device=None):
         cs.search(periods, off, 1e-5, 8, batches, _lib.GTLS_PASS_MAIN, precision, timing=tm, periods_dev=p_dev)
 
     return autotune(run, precision, int(cs.n[c]), int(cs.max_width[c]), device=device)
+
+
+def tune_curve(cur, periods, precision, n_sample=600, batch=50):
+    """``autotune`` for one ``core.CurveOnDevice``: the main pass over every
+    k-th of its sorted trial ``periods`` (host array)."""
+    periods = np.asarray(periods, dtype=np.float64)
+    step = max(1, len(periods) // n_sample)
+    sub = np.ascontiguousarray(periods[::step][:n_sample])
+
+    def run(tm):
+        cur.search(sub, 1e-5, 8, batch, _lib.GTLS_PASS_MAIN, precision, timing=tm)
+
+    return autotune(run, precision, cur.n, cur.maxd, device=cur.device)
