@@ -458,8 +458,11 @@ def bench_batch(args):
         # the plain FP64 per-curve form on the same curves: one gtls().power() each
         torch.cuda.synchronize()
         a = time.perf_counter()
-        ref64 = [gtls(t, y, verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device)
-                 for (t, y) in curves]
+        # same duration-union batch sizes as the batched run (the reference's
+        # free-memory formula gives different ones at different times)
+        ref64 = [gtls(t, y, verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device,
+                                                 batch_periods=int(o.batch_periods))
+                 for (t, y), o in zip(curves, out)]
         torch.cuda.synchronize()
         pc_ms = 1000.0 * (time.perf_counter() - a)
         same = [int(np.argmin(np.abs(p["periods"] - r.period))) == o.period_index
@@ -469,7 +472,8 @@ def bench_batch(args):
                                   "ms": pc_ms, "speedup_of_batched_e2e": pc_ms / e2e_ms,
                                   "best_index_agreement": float(np.mean(same)),
                                   "sde_max_rel_diff": float(np.max(sde_rel)),
-                                  "note": "gtls(t, y).power(precision='fp64') per curve, host arrays, wall clock"}
+                                  "note": "gtls(t, y).power(precision='fp64') per curve with the batched run's "
+                                          "batch sizes, host arrays, wall clock"}
     line["clocks"] = clk.summary()
     if not args.no_cpu_baseline:
         from gtls_b200 import validate as V

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libgtls_b200.so")
 ABI_VERSION = 1
 GTLS_FP64, GTLS_FP32 = 0, 1
 GTLS_PASS_MAIN, GTLS_PASS_ALL = 0, 1
+GTLS_SEARCH_ALL_DURATIONS = 1
 MAX_DURATIONS = 1024
 
 _lib = None
@@ -80,7 +81,7 @@ class SearchDesc(ctypes.Structure):
         ("skip_point", ctypes.c_int32),
         ("batch", ctypes.c_int32),
         ("span", ctypes.c_float),
-        ("reserved", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
         ("chi2_out", ctypes.c_void_p),
         ("loc_out", ctypes.c_void_p),
         ("timing", ctypes.c_void_p),
@@ -120,7 +121,7 @@ class BatchDesc(ctypes.Structure):
         ("templates", ctypes.c_void_p),
         ("depth_min", ctypes.c_double),
         ("skip_point", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
         ("chi2_out", ctypes.c_void_p),
         ("loc_out", ctypes.c_void_p),
         ("timing", ctypes.c_void_p),
@@ -267,7 +268,7 @@ def get_tuning(device=0):
 
 
 def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precision, device=0,
-           want_loc=True, timing=None):
+           want_loc=True, timing=None, flags=0):
     """Run gtls_search for one curve.
 
     ``curve``: dict of device tensors t, y, dy (float64) and ``span`` (float).
@@ -303,13 +304,14 @@ def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precisio
     d.chi2_out = chi2.data_ptr()
     d.loc_out = loc.data_ptr() if loc is not None else None
     d.timing = ctypes.addressof(timing) if timing is not None else None
+    d.flags = int(flags)
     rc = load().gtls_search(ctx, ctypes.byref(d), _stream(torch, device))
     _check(rc, ctx, "gtls_search")
     return chi2, loc
 
 
 def search_batch(curves, periods, period_off, tables, depth_min, skip_point, batches, pass_, precision,
-                 device=0, want_loc=True, timing=None):
+                 device=0, want_loc=True, timing=None, flags=0):
     """Run gtls_search_batch over many curves.
 
     ``curves``: dict of concatenated device tensors t, y, dy (float64), host
@@ -360,6 +362,7 @@ def search_batch(curves, periods, period_off, tables, depth_min, skip_point, bat
     d.chi2_out = chi2.data_ptr()
     d.loc_out = loc.data_ptr() if loc is not None else None
     d.timing = ctypes.addressof(timing) if timing is not None else None
+    d.flags = int(flags)
     rc = load().gtls_search_batch(ctx, ctypes.byref(d), _stream(torch, device))
     _check(rc, ctx, "gtls_search_batch")
     return chi2, loc

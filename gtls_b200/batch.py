@@ -10,8 +10,10 @@ The per-curve steps between the passes (outlier mask, spectra, candidate
 choice) and the host statistics of the best period stay per curve.
 
 The reference has no batched form; it searches one curve per ``gtls``
-object.  ``precision`` defaults to "fp32" here (FP32 chi2 with compensated
-prefix sums in the main pass, every re-search in FP64).
+object.  ``precision`` defaults to "fp32" here (FP32 chi2 with float-float
+prefix sums in the main pass and the candidate re-search, then an FP64
+re-check of each curve's best 32 candidates; harmonics and the best period in
+FP64).
 """
 import types
 
@@ -71,6 +73,19 @@ class CurveSetOnDevice:
 
     def __len__(self):
         return len(self.prepared)
+
+    def curve_view(self, c):
+        """Curve ``c`` as the (curve, tables) dicts of a single-curve ``_lib.search``
+        (views of the concatenated device arrays, no copies)."""
+        a, b = int(self.sample_off[c]), int(self.sample_off[c + 1])
+        d0, d1 = int(self.dur_off[c]), int(self.dur_off[c + 1])
+        mw = int(self.max_width[c])
+        t0 = int(self.tmpl_off[c])
+        curve = dict(t=self.curves["t"][a:b], y=self.curves["y"][a:b], dy=self.curves["dy"][a:b],
+                     span=float(self.span[c]))
+        tables = dict(widths=self.tables["widths"][d0:d1], overshoot=self.tables["overshoot"][d0:d1],
+                      templates=self.tables["templates"][t0:t0 + (d1 - d0) * mw].view(d1 - d0, mw), max_width=mw)
+        return curve, tables
 
     def search(self, periods, period_off, depth_min, skip_point, batches, pass_, precision, want_loc=False,
                timing=None, periods_dev=None):
@@ -173,6 +188,63 @@ class gtls_batch(object):
         return search_subset(list(range(len(self.curves))))
 
 
+def _recheck_fp64(cs, cand, cand_p, c_off, spectra, chi2_dev, p_off, S, depth_min, skip, torch):
+    """FP64 re-check of every curve's best ``core.FP64_RECHECK`` candidates
+    (``core.recheck_plan``), as one batched FP64 search: entry c of the call
+    is curve c restricted to its re-checked candidates and their batch's
+    duration union (a curve whose re-checked candidates span several batches
+    of the candidate list adds one more single-curve call per extra batch)."""
+    dev = cs.dev
+    C = len(cs)
+    plans = []
+    for c in range(C):
+        if len(cand[c]) == 0:
+            plans.append([])
+            continue
+        _, _, power_dev, _, _ = spectra(c)
+        ci = torch.as_tensor(cand[c], device=dev)
+        plans.append(core.recheck_plan(cand_p[c_off[c]:c_off[c + 1]], _d2h(power_dev[ci]), cs.prepared[c]["widths"],
+                                       float(cs.span[c]), int(cs.n[c]), int(S[c]), cs.device))
+    # first batch of every curve's plan in one call
+    widths, overshoot, templ, periods, dur_n, tmpl_n, per_n, gidx = [], [], [], [], [], [], [], []
+    for c in range(C):
+        d0 = int(cs.dur_off[c])
+        mw = int(cs.max_width[c])
+        t0 = int(cs.tmpl_off[c])
+        if plans[c]:
+            sel, union = plans[c][0]
+        else:
+            sel, union = np.zeros(0, dtype=np.int64), np.zeros(1, dtype=np.int64)   # no periods: any duration
+        u = torch.as_tensor(union, device=dev)
+        widths.append(cs.tables["widths"][d0 + u])
+        overshoot.append(cs.tables["overshoot"][d0 + u])
+        rows = cs.tables["templates"][t0:t0 + (int(cs.dur_off[c + 1]) - d0) * mw].view(-1, mw)
+        templ.append(rows[u].reshape(-1))
+        dur_n.append(len(union))
+        tmpl_n.append(len(union) * mw)
+        periods.append(cand_p[c_off[c]:c_off[c + 1]][sel])
+        per_n.append(len(sel))
+        gidx.append(cand[c][sel] + p_off[c])
+    if sum(per_n):
+        tables = dict(widths=torch.cat(widths).contiguous(), overshoot=torch.cat(overshoot).contiguous(),
+                      templates=torch.cat(templ).contiguous(), dur_off=_offsets(dur_n),
+                      tmpl_off=_offsets(tmpl_n)[:-1], max_width=cs.max_width)
+        pc = np.concatenate(periods)
+        c64, _ = _lib.search_batch(cs.curves, _h2d(torch, pc, dev), _offsets(per_n), tables, depth_min, skip,
+                                   np.maximum(np.array(per_n), 1).astype(np.int32), _lib.GTLS_PASS_ALL, "fp64",
+                                   device=cs.device, want_loc=False, flags=_lib.GTLS_SEARCH_ALL_DURATIONS)
+        chi2_dev[_h2d(torch, np.concatenate(gidx), dev)] = c64
+    # further batches (rare): one single-curve call each
+    for c in range(C):
+        for sel, union in plans[c][1:]:
+            curve_c, tables_c = cs.curve_view(c)
+            ch, _ = _lib.search(curve_c, _h2d(torch, cand_p[c_off[c]:c_off[c + 1]][sel], dev),
+                                core.subset_tables(tables_c, union, torch), depth_min, skip, len(sel),
+                                _lib.GTLS_PASS_ALL, "fp64", device=cs.device, want_loc=False,
+                                flags=_lib.GTLS_SEARCH_ALL_DURATIONS)
+            chi2_dev[_h2d(torch, cand[c][sel] + p_off[c], dev)] = ch
+
+
 def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None, autotune=False):
     """The batched search of curves already prepared by ``prepare_curve``.
 
@@ -224,7 +296,9 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
         a, b = int(p_off[c]), int(p_off[c + 1])
         return core._spectra(chi2_dev[a:b], mask_dev[a:b], osf, device)
 
-    # candidates of every curve, re-searched at every start in FP64
+    # candidates of every curve re-searched at every start: in FP64, or (FP32
+    # form) in FP32 followed by an FP64 re-check of each curve's best
+    # core.FP64_RECHECK candidates over their batch's duration union
     cand = []
     for c in range(C):
         a, b = int(p_off[c]), int(p_off[c + 1])
@@ -232,10 +306,13 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
         cand.append(core._candidates(power_dev, mask_dev[a:b], periods_dev[a:b], torch))
     c_off = _offsets([len(x) for x in cand])
     cand_p = np.concatenate([prepared[c]["periods"][cand[c]] for c in range(C)])
-    again, _ = cs.search(cand_p, c_off, depth_min, skip, S, _lib.GTLS_PASS_ALL, "fp64")
+    fp32 = opts.precision == "fp32"
+    again, _ = cs.search(cand_p, c_off, depth_min, skip, S, _lib.GTLS_PASS_ALL, "fp32" if fp32 else "fp64")
     gidx = _h2d(torch, np.concatenate([cand[c] + p_off[c] for c in range(C)]), dev)
     chi2_dev[gidx] = again
     mask_dev[gidx] = 0
+    if fp32:
+        _recheck_fp64(cs, cand, cand_p, c_off, spectra, chi2_dev, p_off, S, depth_min, skip, torch)
     period = np.empty(C)
     h_idx = []
     for c in range(C):

@@ -83,7 +83,8 @@ class CurveOnDevice:
             max_width=self.maxd,
         )
 
-    def search(self, periods, depth_min, skip_point, batch, pass_, precision, want_loc=False, timing=None):
+    def search(self, periods, depth_min, skip_point, batch, pass_, precision, want_loc=False, timing=None,
+               tables=None, flags=0):
         torch = self.torch
         if isinstance(periods, torch.Tensor):
             p = periods.to(self.dev, dtype=torch.float64).contiguous()
@@ -93,8 +94,58 @@ class CurveOnDevice:
         if not pmin > 0 or self.t_max / pmin >= 2.0 ** 31:
             # the fold truncates t/P to a 32-bit int (GPUFun.py:39)
             raise ValueError("periods must be > 0 and max|t| / min(period) < 2^31")
-        return _lib.search(self.curve, p, self.tables, depth_min, skip_point, batch, pass_, precision,
-                           device=self.device, want_loc=want_loc, timing=timing)
+        return _lib.search(self.curve, p, self.tables if tables is None else tables, depth_min, skip_point, batch,
+                           pass_, precision, device=self.device, want_loc=want_loc, timing=timing, flags=flags)
+
+
+# candidates re-evaluated in FP64 after the FP32 form's candidate re-search
+FP64_RECHECK = 32
+
+
+def subset_tables(tables, idx, torch):
+    """The duration tables restricted to the durations ``idx`` (ascending)."""
+    ii = torch.as_tensor(np.asarray(idx, dtype=np.int64), device=tables["widths"].device)
+    return dict(widths=tables["widths"][ii].contiguous(), overshoot=tables["overshoot"][ii].contiguous(),
+                templates=tables["templates"][ii].contiguous(), max_width=tables["max_width"])
+
+
+def recheck_plan(cand_p, power_cand, widths, span, n, batch, device, k=FP64_RECHECK):
+    """Which candidates the FP32 form re-checks in FP64, and over which durations.
+
+    The candidate re-search groups the candidate list in batches of
+    ``batch`` and searches each candidate over its batch's duration union
+    (core.py:1081-1115).  The ``k`` candidates of highest power (``power_cand``,
+    host, in candidate-list order) are re-searched in FP64 over exactly their
+    batch's union (``GTLS_SEARCH_ALL_DURATIONS`` with the union's durations),
+    so that each gets the value an FP64 re-search of the whole list gives.
+    Returns a list of (positions in the candidate list, union duration
+    indices), one entry per batch that holds re-checked candidates."""
+    if len(cand_p) == 0:
+        return []
+    key = np.where(np.isfinite(power_cand), -power_cand, np.inf)
+    top = np.argsort(key, kind="stable")[:k]
+    wmin, wmax = _lib.duration_ranges(np.asarray(cand_p, dtype=np.float64), span, n, device=device)
+    valid = (widths[None, :] >= wmin[:, None]) & (widths[None, :] <= wmax[:, None])
+    group = np.arange(len(cand_p)) // batch
+    plan = []
+    for g in np.unique(group[top]):
+        union = np.nonzero(valid[group == g].any(axis=0))[0]
+        if len(union):
+            plan.append((np.sort(top[group[top] == g]), union))
+    return plan
+
+
+def fp64_recheck(search, cand_p, power_cand, widths, span, n, batch, device, k=FP64_RECHECK):
+    """Run ``recheck_plan``: ``search(periods, union)`` is the FP64 search of
+    those periods over those durations (returns a chi2 tensor).  Returns
+    (positions in the candidate list, their FP64 chi2, host)."""
+    pos_out, val_out = [], []
+    for sel, union in recheck_plan(cand_p, power_cand, widths, span, n, batch, device, k):
+        pos_out.append(sel)
+        val_out.append(_d2h(search(np.asarray(cand_p)[sel], union)))
+    if not pos_out:
+        return np.zeros(0, dtype=np.int64), np.zeros(0)
+    return np.concatenate(pos_out), np.concatenate(val_out)
 
 
 def _spectra(chi2_dev, mask_dev, osf, device):
@@ -185,15 +236,30 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     if fast:
         return mperiods, raw_power
 
-    # candidates re-searched at every phase start, in FP64
+    # candidates re-searched at every phase start: in FP64, or (FP32 form) in
+    # FP32 followed by an FP64 re-check of the best FP64_RECHECK of them
     cand_idx = _candidates(power_dev, mask_dev, periods_dev, torch)
     TRANSFER["d2h"] += cand_idx.nbytes
     cand_p = periods[cand_idx]
-    again, _ = cur.search(cand_p, transit_depth_min, skip, S, _lib.GTLS_PASS_ALL, "fp64")
+    again, _ = cur.search(cand_p, transit_depth_min, skip, S, _lib.GTLS_PASS_ALL,
+                          "fp32" if precision == "fp32" else "fp64")
     ci = _h2d(torch, cand_idx, dev)
     chi2_dev[ci] = again
     mask_dev[ci] = 0
     _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
+    rechecked = np.zeros(0, dtype=np.int64)
+    if precision == "fp32":
+        def search64(p, union):
+            c, _ = cur.search(p, transit_depth_min, skip, len(p), _lib.GTLS_PASS_ALL, "fp64",
+                              tables=subset_tables(cur.tables, union, torch), flags=_lib.GTLS_SEARCH_ALL_DURATIONS)
+            return c
+        pos, val = fp64_recheck(search64, cand_p, _d2h(power_dev[ci]), cur.widths, cur.curve["span"], cur.n, S,
+                                device)
+        if len(pos):
+            chi2_dev[_h2d(torch, cand_idx[pos], dev)] = _h2d(torch, val, dev)
+            _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
+        rechecked = cand_idx[pos]
+        again = chi2_dev[ci]
     pw = power_dev[ci]
     best = int(cand_idx[int(torch.argmax(pw).item())])
     period = periods[best]
@@ -222,6 +288,7 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     power_m = ma.array(power_h, mask=mask_h)
     periods_m = ma.array(periods, mask=mask_h)
     diag = dict(batch_periods=S, period_index=best, sde_raw=sde_raw, again=_d2h(again), chi2_main=chi2_main,
+                fp64_rechecked=rechecked,
                 harmonic_indices=h_idx, chi2_harmonics=_d2h(again2), loc=fin["loc"],
                 skip_point=skip, precision=precision)
     return (periods_m, period, fin["raw_duration"], fin["width"], fin["duration"], fin["depth"], fin["T0"],

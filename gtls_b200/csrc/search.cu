@@ -1041,7 +1041,7 @@ __global__ void duration_range_batch_kernel(const CurveDev<Real>* __restrict__ c
 // the ascending list).
 template <typename Real>
 __global__ void union_kernel(const CurveDev<Real>* __restrict__ cds, const long long* __restrict__ b_off,
-                             int n_curves) {
+                             int n_curves, int all_durations) {
   __shared__ int flags[GTLS_MAX_DURATIONS];
   __shared__ int cost[GTLS_MAX_DURATIONS];
   __shared__ short pos[GTLS_MAX_DURATIONS];
@@ -1056,7 +1056,7 @@ __global__ void union_kernel(const CurveDev<Real>* __restrict__ cds, const long 
     int w = C.widths[d];
     int any = 0;
     for (long long p = p0; p < p1 && !any; ++p) any = (w >= C.wmin[p]) && (w <= C.wmax[p]);
-    flags[d] = any;
+    flags[d] = any || (all_durations && p1 > p0);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1134,7 +1134,7 @@ struct CurveHost {
 
 template <typename Real>
 static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int precision_pass, int skip_point,
-                      double depth_min, gtls_timing* tm, cudaStream_t st) {
+                      double depth_min, int flags, gtls_timing* tm, cudaStream_t st) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
   const bool all = precision_pass == GTLS_PASS_ALL;
@@ -1358,7 +1358,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   if (p_off[n_curves] > 0)
     duration_range_batch_kernel<Real><<<(unsigned)((p_off[n_curves] + 255) / 256), 256, 0, st>>>(d_cd, d_poff,
                                                                                                  n_curves);
-  if (b_off[n_curves] > 0) union_kernel<Real><<<(unsigned)b_off[n_curves], 256, 0, st>>>(d_cd, d_boff, n_curves);
+  if (b_off[n_curves] > 0)
+    union_kernel<Real><<<(unsigned)b_off[n_curves], 256, 0, st>>>(d_cd, d_boff, n_curves,
+                                                                   (flags & GTLS_SEARCH_ALL_DURATIONS) ? 1 : 0);
   template_rows_kernel<Real><<<(unsigned)d_off[n_curves], 256, 0, st>>>(d_cd, d_doff, n_curves);
   ctx->launches += 4;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
@@ -1471,6 +1473,7 @@ extern "C" int gtls_search(gtls_ctx* ctx, const gtls_search_desc* d, void* strea
   if (d->n_periods < 1) return fail(ctx, GTLS_E_INVALID, "n_periods >= 1 required");
   if (d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "skip_point must be >= 1");
   if (d->pass != GTLS_PASS_MAIN && d->pass != GTLS_PASS_ALL) return fail(ctx, GTLS_E_INVALID, "unknown pass");
+  if (d->flags & ~GTLS_SEARCH_ALL_DURATIONS) return fail(ctx, GTLS_E_INVALID, "unknown flags");
   CurveHost h;
   h.t = d->t;
   h.y = d->y;
@@ -1491,8 +1494,10 @@ extern "C" int gtls_search(gtls_ctx* ctx, const gtls_search_desc* d, void* strea
   if (rc) return rc;
   GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (d->precision == GTLS_FP64) return run_search<double>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->timing, st);
-  if (d->precision == GTLS_FP32) return run_search<float>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->timing, st);
+  if (d->precision == GTLS_FP64)
+    return run_search<double>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->flags, d->timing, st);
+  if (d->precision == GTLS_FP32)
+    return run_search<float>(ctx, &h, 1, d->pass, d->skip_point, d->depth_min, d->flags, d->timing, st);
   return fail(ctx, GTLS_E_INVALID, "unknown precision");
 }
 
@@ -1504,6 +1509,7 @@ extern "C" int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* d, void* 
     return fail(ctx, GTLS_E_INVALID, "null host array or no curves");
   if (d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "skip_point must be >= 1");
   if (d->pass != GTLS_PASS_MAIN && d->pass != GTLS_PASS_ALL) return fail(ctx, GTLS_E_INVALID, "unknown pass");
+  if (d->flags & ~GTLS_SEARCH_ALL_DURATIONS) return fail(ctx, GTLS_E_INVALID, "unknown flags");
   std::vector<CurveHost> hs(d->n_curves);
   for (int c = 0; c < d->n_curves; ++c) {
     CurveHost& h = hs[c];
@@ -1533,9 +1539,11 @@ extern "C" int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* d, void* 
   GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (d->precision == GTLS_FP64)
-    return run_search<double>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->timing, st);
+    return run_search<double>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->flags,
+                              d->timing, st);
   if (d->precision == GTLS_FP32)
-    return run_search<float>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->timing, st);
+    return run_search<float>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->flags,
+                             d->timing, st);
   return fail(ctx, GTLS_E_INVALID, "unknown precision");
 }
 

@@ -7,7 +7,8 @@ one entry is accepted and runs on the first device: the reference's own
 multi-GPU mode (worker processes per GPU) is replaced by ``distributed``
 below, with one process per GPU started by torchrun.
 Extra keywords: ``precision`` ("fp64" plain FP64 search, default; "fp32" FP32
-chi2 with compensated prefix sums and FP64 re-search of the candidates),
+chi2 with float-float prefix sums in the main pass and the candidate
+re-search, then an FP64 re-check of the 32 best candidates),
 ``batch_periods`` (periods per duration-union batch; default: the reference's
 free-memory formula, core.py:620-628) and ``distributed`` (shard the main pass
 over the ranks of the initialised torch.distributed process group, one

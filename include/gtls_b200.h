@@ -158,13 +158,20 @@ typedef struct gtls_search_desc {
   int32_t skip_point;         /* int(1/T0_fit_margin) or 0x7f800000             */
   int32_t batch;              /* periods per duration-union batch, >= 1         */
   float span;                 /* max(t) - min(t) as float                       */
-  int32_t reserved;
+  int32_t flags;              /* 0, or GTLS_SEARCH_ALL_DURATIONS                */
   double* chi2_out;           /* [n_periods]                                    */
   int64_t* loc_out;           /* [n_periods] or NULL                            */
   gtls_timing* timing;        /* host, or NULL                                  */
 } gtls_search_desc;
 
 #define GTLS_MAX_DURATIONS 1024
+
+/* flags: search every given duration for every period, instead of the
+ * durations valid for at least one period of its batch.  With it a caller
+ * re-searches a few periods of a batch with that batch's own duration union
+ * (computed from all its periods), e.g. to re-check candidates in another
+ * precision.  No counterpart in the reference. */
+#define GTLS_SEARCH_ALL_DURATIONS 1
 
 int gtls_search(gtls_ctx* ctx, const gtls_search_desc* desc, void* stream);
 
@@ -203,7 +210,7 @@ typedef struct gtls_batch_desc {
   const double* templates;    /* device, all curves' template rows              */
   double depth_min;
   int32_t skip_point;
-  int32_t reserved;
+  int32_t flags;              /* 0, or GTLS_SEARCH_ALL_DURATIONS                */
   double* chi2_out;           /* device, all curves' periods                    */
   int64_t* loc_out;           /* device or NULL                                 */
   gtls_timing* timing;        /* host, or NULL                                  */

@@ -180,3 +180,43 @@ def test_spectra_matches_reference_stats(cuda):
         np.testing.assert_allclose(SR.cpu().numpy()[~m], sp["case%d_SR" % i][~m], rtol=1e-12)
         np.testing.assert_allclose(power.cpu().numpy()[~m], sp["case%d_power" % i][~m], rtol=1e-9, atol=1e-9)
         np.testing.assert_allclose([sde_raw, sde], sp["case%d_sde" % i], rtol=1e-9)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_all_durations_flag_reproduces_a_batch_union(cuda, precision):
+    """Re-searching some periods of a batch over that batch's duration union
+    (GTLS_SEARCH_ALL_DURATIONS) gives exactly their values in the full search."""
+    import torch
+    from gtls_b200 import _lib
+    from gtls_b200.core import subset_tables
+    s = search_inputs(seed=33, n=1200, span=6.0, use_dy=True)
+    cur = _curve(s)
+    P = s["periods"][::17][:21]
+    S = 7
+    full, floc = cur.search(P, 1e-5, 8, S, _lib.GTLS_PASS_ALL, precision, want_loc=True)
+    full, floc = full.cpu().numpy(), floc.cpu().numpy()
+    span = s["t"].max() - s["t"].min()
+    wmin, wmax = O.duration_ranges(P, span, len(s["t"]))
+    valid = (s["widths"][None, :] >= wmin[:, None]) & (s["widths"][None, :] <= wmax[:, None])
+    for b, sub in [(0, [3, 5]), (1, [7]), (2, [14, 15, 20])]:
+        union = np.nonzero(valid[b * S:(b + 1) * S].any(axis=0))[0]
+        c, l = cur.search(P[sub], 1e-5, 8, len(sub), _lib.GTLS_PASS_ALL, precision, want_loc=True,
+                          tables=subset_tables(cur.tables, union, torch), flags=_lib.GTLS_SEARCH_ALL_DURATIONS)
+        np.testing.assert_array_equal(c.cpu().numpy(), full[sub])
+        np.testing.assert_array_equal(l.cpu().numpy(), floc[sub])
+
+
+def test_fp32_form_rechecks_its_best_candidates_in_fp64(cuda):
+    from gtls_b200 import gtls, synthetic
+    t, y, _ = synthetic.small_curve(seed=34, n=2500, span=9.0, period=1.7, depth=5e-3)
+    kw = dict(oversampling_factor=2, batch_periods=40, use_threads=1)
+    r32 = gtls(t, y, verbose=False).power(precision="fp32", **kw)
+    r64 = gtls(t, y, verbose=False).power(precision="fp64", **kw)
+    re = np.asarray(r32.diagnostics["fp64_rechecked"])
+    assert len(re) == 32
+    assert list(r32.possiblePeriodsIndices) == list(r64.possiblePeriodsIndices)
+    c32 = np.ma.filled(r32.chi2, np.nan)
+    c64 = np.ma.filled(r64.chi2, np.nan)
+    np.testing.assert_array_equal(c32[re], c64[re])
+    assert r32.period == r64.period and r32.durationPoints == r64.durationPoints
+    assert abs(r32.SDE - r64.SDE) <= 1e-6 * abs(r64.SDE)
