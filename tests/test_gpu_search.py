@@ -220,3 +220,24 @@ def test_fp32_form_rechecks_its_best_candidates_in_fp64(cuda):
     np.testing.assert_array_equal(c32[re], c64[re])
     assert r32.period == r64.period and r32.durationPoints == r64.durationPoints
     assert abs(r32.SDE - r64.SDE) <= 1e-6 * abs(r64.SDE)
+
+
+def test_search_rejects_invalid_arguments_and_stays_usable(cuda):
+    from gtls_b200 import _lib
+    s = search_inputs(seed=35, n=600, span=4.0)
+    cur = _curve(s)
+    P = s["periods"][::20]
+    with pytest.raises(_lib.GtlsError, match="flags"):
+        cur.search(P, 1e-5, 8, 3, _lib.GTLS_PASS_MAIN, "fp64", flags=4)
+    with pytest.raises(_lib.GtlsError, match="pass"):
+        cur.search(P, 1e-5, 8, 3, 7, "fp64")
+    with pytest.raises(_lib.GtlsError, match="skip_point"):
+        cur.search(P, 1e-5, 0, 3, _lib.GTLS_PASS_MAIN, "fp64")
+    with pytest.raises(_lib.GtlsError, match="batch"):
+        cur.search(P, 1e-5, 8, 0, _lib.GTLS_PASS_MAIN, "fp64")
+    with pytest.raises(ValueError):
+        cur.search(np.array([0.0, 1.0]), 1e-5, 8, 3, _lib.GTLS_PASS_MAIN, "fp64")
+    c, _ = cur.search(P, 1e-5, 8, 3, _lib.GTLS_PASS_MAIN, "fp64")
+    c_ref, _ = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
+                                s["overshoot"], s["maxd"], 1e-5, 8, 3)
+    np.testing.assert_allclose(c.cpu().numpy(), c_ref, rtol=RTOL64)
