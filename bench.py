@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--accuracy", action="store_true",
                     help="cfg4: only the agreement of the batched FP32 search with the plain FP64 per-curve "
                          "search over the sample (one pass each), no timing steps")
+    ap.add_argument("--tuning", default=None,
+                    help="fixed launch shapes 'tile_cap_fp32,tile_cap_fp64,bucket_shift' instead of autotuning "
+                         "(profiling runs: ncu slows untimed launches, which would skew the tuner)")
     ap.add_argument("--chunk-mb", type=int, default=0,
                     help="per-chunk scratch budget of the searches in MiB (default: the library's 8 GiB)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -254,6 +257,18 @@ CFG4_METRIC = ("light curves/s (batched TLS search of the 4,096-curve synthetic 
                "27-1,470 d, per-curve Ofir grids and duration grids)")
 
 
+def fixed_or_tuned(args, tune_fn, device):
+    """Launch shapes for the run: ``--tuning`` if given, else chosen by timing
+    on the workload's own data (untimed, before the warm-up).  Sets them on
+    the device's context and returns them."""
+    from gtls_b200 import _lib
+    if args.tuning:
+        c32, c64, shift = (int(v) for v in args.tuning.split(","))
+        _lib.set_tuning(tile_cap_fp32=c32, tile_cap_fp64=c64, bucket_shift=shift, device=device)
+        return _lib.get_tuning(device)
+    return tune_fn()
+
+
 def cfg4_sample(n_curves):
     """Every (4096 / n_curves)-th curve of the 4,096-curve set, and the set's
     total work (sum over curves of samples x trial periods)."""
@@ -383,7 +398,7 @@ def bench_batch(args):
     prepared = [batch.prepare_curve(t, y, None, opts, device=device) for (t, y) in curves]
     cs = batch.CurveSetOnDevice(prepared, device=device)
     from gtls_b200 import tune
-    tuning = tune.tune_curve_set(cs, args.precision)   # launch shapes chosen on this data (untimed)
+    tuning = fixed_or_tuned(args, lambda: tune.tune_curve_set(cs, args.precision), device)
     work = float(sum(len(p["t"]) * len(p["periods"]) for p in prepared))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cs.dev)
     for _ in range(args.warmup):
@@ -649,7 +664,7 @@ def main():
     batch = core.reference_batch_size(len(periods), cur.n, cur.maxd, len(cur.widths), free)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=cur.dev)  # > 126 MB L2
     from gtls_b200 import tune
-    tuning = tune.tune_curve(cur, periods, args.precision)   # launch shapes chosen on this data (untimed)
+    tuning = fixed_or_tuned(args, lambda: tune.tune_curve(cur, periods, args.precision), device)
 
     def one_step(timing=None):
         return core.run_search(cur, periods, periods_dev, t, y, dy, 1e-5, 0.125, kw["oversampling_factor"],
