@@ -467,6 +467,10 @@ def bench_batch(args):
                       ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
     }
     truth = [(specs["period"][i], bool(specs["has_transit"][i])) for i in idx]
+    starts = statistics.mean(t["chi2_starts"] for t in timings)
+    line["trial_evaluations"] = {
+        "what": "(period, duration, start) chi2 evaluations of the main pass per step (the re-searches come on top)",
+        "per_step": starts, "per_s_device": starts / (ms * 1e-3), "per_s_main_pass_kernel": starts / (chi2_ms * 1e-3)}
     line["result"] = {"recovered_1pct": int(sum(abs(r.period - p) < 0.01 * p for r, (p, h) in zip(out, truth) if h)),
                       "with_transit": int(sum(h for _, h in truth))}
     if not args.no_per_curve:
@@ -772,6 +776,11 @@ def main():
         "stages_ms": {k: statistics.mean(tm[k] for tm in timings) for k in
                       ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
         "result": {"period": float(out[1]), "true_period": truth["period"], "SDE": float(out[7])},
+        "trial_evaluations": {
+            "what": "(period, duration, start) chi2 evaluations of the main pass per step (the re-searches come on top)",
+            "per_step": statistics.mean(tm["chi2_starts"] for tm in timings),
+            "per_s_device": statistics.mean(tm["chi2_starts"] for tm in timings) / (ms_per_step * 1e-3),
+            "per_s_main_pass_kernel": statistics.mean(tm["chi2_starts"] for tm in timings) / (chi2_ms * 1e-3)},
     }
     if rank == 0:
         line["clocks"] = clk.summary()
