@@ -361,9 +361,10 @@ def cfg4_once(args, curves, idx, specs, total_work, device):
     tm = _lib.Timing()
     launches0 = _lib.launch_count(device)
     a = time.perf_counter()
+    phases = {}
     with Clocks(device) as clk:
         res = gtls_batch(curves).power(precision=args.precision, use_threads=1, GPUDeviceID=device,
-                                       keep_spectra=False, timing=tm)
+                                       keep_spectra=False, timing=tm, phases=phases)
         torch.cuda.synchronize()
     sec = time.perf_counter() - a
     work = float(sum(len(c[0]) * G.ofir_coefficients(1.0, 1.0, np.ptp(c[0]))[2] for c in curves))
@@ -374,6 +375,7 @@ def cfg4_once(args, curves, idx, specs, total_work, device):
                        "precision": args.precision, "timing": "wall clock around gtls_batch(curves).power() from "
                                                              "host arrays (grids, templates, uploads included)"},
             "main_pass_stages_ms": {k: tm.as_dict()[k] for k in ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
+            "phases_s": phases,
             "gpu_launches": int(_lib.launch_count(device) - launches0),
             "result": {"recovered_1pct": int(sum(abs(r.period - specs["period"][i]) < 0.01 * specs["period"][i]
                                                  for r, i in zip(res, idx) if specs["has_transit"][i])),

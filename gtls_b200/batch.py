@@ -131,6 +131,30 @@ def prepare_curve(t, y, dy, opts, device=0):
                 durations=durs, tmpl=tmpl, maxd=int(maxd), duration_grid=np.asarray(durations))
 
 
+class _Phases:
+    """Wall-clock time per phase of a batched search (a dict given by the
+    caller), with a device synchronisation at each boundary; no-op when the
+    caller gives none."""
+
+    def __init__(self, out):
+        self.out = out
+        self.t = None
+        if out is not None:
+            import time
+            import torch
+            self._time, self._sync = time.perf_counter, torch.cuda.synchronize
+            self._sync()
+            self.t = self._time()
+
+    def mark(self, name):
+        if self.out is None:
+            return
+        self._sync()
+        now = self._time()
+        self.out[name] = self.out.get(name, 0.0) + (now - self.t)
+        self.t = now
+
+
 def _offsets(counts):
     return np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
 
@@ -160,6 +184,7 @@ class gtls_batch(object):
         autotune = bool(kwargs.pop("autotune", True))
         keep_spectra = bool(kwargs.pop("keep_spectra", True))
         timing = kwargs.pop("timing", None)
+        phases = kwargs.pop("phases", None)
         kwargs.setdefault("precision", "fp32")
         opts = types.SimpleNamespace()
         opts, kwargs = validate_args(opts, kwargs)
@@ -175,9 +200,11 @@ class gtls_batch(object):
             if per_curve_batch:
                 sub = types.SimpleNamespace(**vars(opts))
                 sub.batch_periods = np.asarray(opts.batch_periods)[list(indices)]
+            ph = _Phases(phases)
             prepared = [prepare_curve(*self.curves[i], sub, device=device) for i in indices]
+            ph.mark("prepare_curves")
             return search_prepared(prepared, sub, device=device, full_stats=full_stats,
-                                   keep_spectra=keep_spectra, timing=timing, autotune=autotune)
+                                   keep_spectra=keep_spectra, timing=timing, autotune=autotune, phases=phases)
 
         if opts.distributed:
             # each rank searches a share of the curves balanced by estimated
@@ -245,7 +272,8 @@ def _recheck_fp64(cs, cand, cand_p, c_off, spectra, chi2_dev, p_off, S, depth_mi
             chi2_dev[_h2d(torch, cand[c][sel] + p_off[c], dev)] = ch
 
 
-def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None, autotune=False):
+def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=True, timing=None, autotune=False,
+                    phases=None):
     """The batched search of curves already prepared by ``prepare_curve``.
 
     Returns one ``types.SimpleNamespace`` per curve with period, duration,
@@ -253,16 +281,21 @@ def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=Tru
     ``keep_spectra``) periods, power and chi2 as masked arrays.  With
     ``autotune`` the launch shapes are first tuned on the set's largest
     curve (``tune.tune_curve_set``; cached per shape, results unchanged)."""
+    ph = _Phases(phases)
     cs = CurveSetOnDevice(prepared, device=device)
+    ph.mark("upload")
     if autotune:
         from . import tune
         tune.tune_curve_set(cs, opts.precision)
-    return search_on_device(cs, opts, full_stats=full_stats, keep_spectra=keep_spectra, timing=timing)
+        ph.mark("tune")
+    return search_on_device(cs, opts, full_stats=full_stats, keep_spectra=keep_spectra, timing=timing, phases=phases)
 
 
-def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None):
-    """The batched search of a ``CurveSetOnDevice`` (see ``search_prepared``)."""
+def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None, phases=None):
+    """The batched search of a ``CurveSetOnDevice`` (see ``search_prepared``).
+    ``phases``: optional dict receiving the wall-clock seconds of each phase."""
     import torch
+    ph = _Phases(phases)
     prepared = cs.prepared
     device = cs.device
     dev = cs.dev
@@ -285,6 +318,7 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
     # main pass
     chi2_dev, _ = cs.search(periods_h, p_off, depth_min, skip, S, _lib.GTLS_PASS_MAIN, opts.precision,
                             timing=timing, periods_dev=periods_dev)
+    ph.mark("main_pass")
     raw_chi2 = _d2h(chi2_dev)
     mask = np.zeros(len(raw_chi2), dtype=bool)
     for c in range(C):
@@ -307,12 +341,15 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
     c_off = _offsets([len(x) for x in cand])
     cand_p = np.concatenate([prepared[c]["periods"][cand[c]] for c in range(C)])
     fp32 = opts.precision == "fp32"
+    ph.mark("mask_spectra_candidates")
     again, _ = cs.search(cand_p, c_off, depth_min, skip, S, _lib.GTLS_PASS_ALL, "fp32" if fp32 else "fp64")
     gidx = _h2d(torch, np.concatenate([cand[c] + p_off[c] for c in range(C)]), dev)
     chi2_dev[gidx] = again
     mask_dev[gidx] = 0
+    ph.mark("candidate_research")
     if fp32:
         _recheck_fp64(cs, cand, cand_p, c_off, spectra, chi2_dev, p_off, S, depth_min, skip, torch)
+        ph.mark("fp64_recheck")
     period = np.empty(C)
     h_idx = []
     for c in range(C):
@@ -323,6 +360,7 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
         idx, _ = core.find_nearest_indices([P * r for r in (0.5, 1, 2, 2 / 3, 3 / 2)], prepared[c]["periods"])
         h_idx.append(idx)
 
+    ph.mark("best_candidate")
     # harmonics
     h_off = _offsets([len(x) for x in h_idx])
     h_p = np.concatenate([prepared[c]["periods"][h_idx[c]] for c in range(C)])
@@ -330,6 +368,7 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
     gidx = _h2d(torch, np.concatenate([h_idx[c] + p_off[c] for c in range(C)]), dev)
     chi2_dev[gidx] = again2
     mask_dev[gidx] = 0
+    ph.mark("harmonics_research")
     best_idx = np.empty(C, dtype=np.int64)
     sde = np.empty(C)
     sde_raw = np.empty(C)
@@ -342,10 +381,12 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
         if keep_spectra:
             power_all.append(power_dev)
 
+    ph.mark("spectra_best_harmonic")
     # best period of every curve at every start and duration of its range
     one = np.ones(C, dtype=np.int32)
     chi2_b, loc_b = cs.search(period, _offsets(one), depth_min, 1, one, _lib.GTLS_PASS_ALL, "fp64", want_loc=True)
     loc_h = _d2h(loc_b)
+    ph.mark("best_period_search")
     chi2_bh = _d2h(chi2_b)
     chi2_h = _d2h(chi2_dev) if keep_spectra else None
     mask_h = _d2h(mask_dev).astype(bool) if keep_spectra else None
@@ -369,4 +410,5 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None)
             r.chi2 = np.ma.array(chi2_h[a:b], mask=m)
             r.chi2_main = raw_chi2[a:b]
         out.append(r)
+    ph.mark("finish_host")
     return out
