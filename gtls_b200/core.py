@@ -331,12 +331,13 @@ def finish_period(widths, durations, overshoot, maxd, span, period, loc, t, y, d
     mean = best_y[k0:k0 + width].mean()
     depth = float((1 - mean) * ovs)
     tx = best_t[k0]
-    T0 = tx - int((tx - min(t)) / period) * period - period
+    t_min = float(np.min(t))
+    T0 = tx - int((tx - t_min) / period) * period - period
     dur_days = float(stats.calc_duration_days(t, period, T0, raw_duration))
     out = dict(raw_duration=raw_duration, width=width, duration=dur_days, depth=depth, loc=loc)
     if not full_stats:
         T0 = T0 + dur_days / 2
-        if T0 < min(t):
+        if T0 < t_min:
             T0 = T0 + period
         out["T0"] = float(T0)
         return out
@@ -348,7 +349,7 @@ def finish_period(widths, durations, overshoot, maxd, span, period, loc, t, y, d
     snr_fit_pink = (1 - depth) / ((np.std(out_tr) ** 2 / width) + (red ** 2 / len(transit_times))) ** 0.5
     T0 = T0 + dur_days / 2
     transit_times = transit_times + dur_days / 2
-    if T0 < min(t):
+    if T0 < t_min:
         T0 = T0 + period
     d_odd, d_even, s_odd, s_even, f_odd, f_even, per_count, _, _ = stats.intransit_stats(
         t, y, transit_times, dur_days)

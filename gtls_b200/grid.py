@@ -35,8 +35,9 @@ def T14(R_s, M_s, P, upper_limit=constants.FRACTIONAL_TRANSIT_DURATION_MAX, smal
 
 def duration_grid(periods, shortest, log_step=constants.DURATION_GRID_STEP):
     """Log-spaced fractional durations between the T14 bounds (grid.py:32-53)."""
-    duration_max = T14(R_s=constants.R_STAR_MAX, M_s=constants.M_STAR_MAX, P=min(periods), small=False)
-    duration_min = T14(R_s=constants.R_STAR_MIN, M_s=constants.M_STAR_MIN, P=max(periods), small=True)
+    periods = np.asarray(periods, dtype=np.float64)   # min/max of an array: NumPy's, same values
+    duration_max = T14(R_s=constants.R_STAR_MAX, M_s=constants.M_STAR_MAX, P=float(np.min(periods)), small=False)
+    duration_min = T14(R_s=constants.R_STAR_MIN, M_s=constants.M_STAR_MIN, P=float(np.max(periods)), small=True)
     durations = [duration_min]
     current = duration_min
     while current * log_step < duration_max:

@@ -14,7 +14,7 @@ def transit_mask(t, period, duration, T0):
 
 
 def all_transit_times(T0, t, period):
-    transit_times = [T0 + period] if T0 < min(t) else [T0]
+    transit_times = [T0 + period] if T0 < np.min(t) else [T0]
     prev = transit_times[0]
     end = np.min(t) + (np.max(t) - np.min(t))
     while True:

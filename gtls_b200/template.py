@@ -98,16 +98,25 @@ def get_cache(durations, maxwidth_in_samples, per, rp, a, inc, ecc, w, u, limb_d
                                      ("overshoot", "f8")])
     ref = reference_transit(maxwidth_in_samples, per, rp, a, inc, ecc, w, u, limb_dark)
     dmax = np.max(durations)
+    samples = maxwidth_in_samples
+    reference_time = np.linspace(-0.5, 0.5, samples)
+    cutoff = 1 - constants.NUMERICAL_STABILITY_CUTOFF
     lc_arr = []
     for row, duration in enumerate(durations):
-        scaled = fractional_transit(duration, dmax, constants.SIGNAL_DEPTH, maxwidth_in_samples, ref)
+        # the in-transit part of fractional_transit(duration, dmax, SIGNAL_DEPTH,
+        # samples, ref): its padding is 1 - (1 - 1) * depth = 1 exactly, never
+        # below the cutoff, so the trimmed signal comes from the squeezed
+        # template alone (same values, no padded array built)
+        occupied = int((duration / dmax) * samples)
+        y_new = interp_linear(np.linspace(-0.5, 0.5, occupied), reference_time, ref)
+        scaled = 1 - ((1 - y_new) * constants.SIGNAL_DEPTH)
         overview["duration"][row] = duration
         overview["width_in_samples"][row] = int((duration / dmax) * maxwidth_in_samples)
-        full = np.where(scaled < (1 - constants.NUMERICAL_STABILITY_CUTOFF))
+        full = np.nonzero(scaled < cutoff)[0]
         if np.size(full) == 0:
             raise ValueError("transit template of duration %g has no in-transit samples "
                              "(light curve too short for this duration grid)" % duration)
-        signal = scaled[np.min(full): np.max(full) + 1]
+        signal = scaled[full[0]: full[-1] + 1]
         lc_arr.append(signal)
         overview["overshoot"][row] = 1 / (2 - np.mean(signal) / np.min(signal))
     lc = np.empty(len(lc_arr), dtype=object)
