@@ -93,3 +93,29 @@ def test_candidate_selection_matches_reference_sort():
         ours = _candidates(torch.from_numpy(power), torch.zeros(n, dtype=torch.uint8), torch.from_numpy(periods),
                            torch)
         assert list(ours) == list(idx)
+
+
+def test_fp64_recheck_plan_uses_each_batch_union(monkeypatch):
+    """The FP32 form re-checks its best candidates over exactly the duration
+    union of their batch of the candidate list (core.py:1081-1115 groups the
+    candidates in batches of S)."""
+    import tls_oracle as O
+    from gtls_b200 import _lib, core
+    monkeypatch.setattr(_lib, "duration_ranges", lambda p, span, n, device=0: O.duration_ranges(np.asarray(p), span, n))
+    rng = np.random.default_rng(5)
+    cand_p = np.exp(rng.uniform(np.log(0.6), np.log(300.0), 60))
+    power = rng.normal(size=60)
+    power[7] = np.nan
+    widths = np.unique(rng.integers(5, 4000, 40)).astype(np.int64)
+    n, span, S = 20000, np.float32(800.0), 25
+    plan = core.recheck_plan(cand_p, power, widths, span, n, S, device=0, k=10)
+    chosen = np.sort(np.concatenate([sel for sel, _ in plan]))
+    order = np.argsort(np.where(np.isfinite(power), -power, np.inf), kind="stable")
+    np.testing.assert_array_equal(chosen, np.sort(order[:10]))
+    wmin, wmax = O.duration_ranges(cand_p, span, n)
+    valid = (widths[None, :] >= wmin[:, None]) & (widths[None, :] <= wmax[:, None])
+    for sel, union in plan:
+        g = sel[0] // S
+        assert np.all(sel // S == g)
+        np.testing.assert_array_equal(union, np.nonzero(valid[g * S:(g + 1) * S].any(axis=0))[0])
+    assert 7 not in chosen
