@@ -143,6 +143,8 @@ EXPORTS = {
     "gtls_duration_ranges": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_int32,
                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "gtls_search": ([ctypes.c_void_p, ctypes.POINTER(SearchDesc), ctypes.c_void_p], ctypes.c_int),
+    "gtls_fold_order": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+                         ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "gtls_search_batch": ([ctypes.c_void_p, ctypes.POINTER(BatchDesc), ctypes.c_void_p], ctypes.c_int),
     "gtls_spectra": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
@@ -249,6 +251,20 @@ def set_chunk_budget(nbytes, device=0):
     """Per-chunk scratch budget of the searches on ``device`` (bytes)."""
     ctx = context(device)
     _check(load().gtls_set_chunk_budget(ctx, int(nbytes)), ctx, "gtls_set_chunk_budget")
+
+
+def fold_order(t, periods, device=0):
+    """gtls_fold_order: the stable phase order of device float64 tensor ``t``
+    for every period of device float64 tensor ``periods``; returns an int32
+    tensor [len(periods), len(t)]."""
+    torch = _torch()
+    ctx = context(device)
+    n, npd = int(t.numel()), int(periods.numel())
+    out = torch.empty((npd, n), dtype=torch.int32, device=t.device)
+    rc = load().gtls_fold_order(ctx, t.data_ptr(), n, periods.data_ptr(), npd, out.data_ptr(),
+                                _stream(torch, device))
+    _check(rc, ctx, "gtls_fold_order")
+    return out
 
 
 def set_tuning(tile_cap_fp32=0, tile_cap_fp64=0, bucket_shift=0, device=0):

@@ -281,11 +281,14 @@ __device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot,
   }
 }
 
-template <typename Real>
+// kOrder: write only the stable fold order of each period (order_out[rec_off
+// + local * n + p] = original index of sorted position p) instead of the
+// records and prefix (gtls_fold_order).
+template <typename Real, bool kOrder = false>
 __global__ void __launch_bounds__(kPrepThreads)
 prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
                uint2* __restrict__ scr_slot, typename Tr<Real>::R2* __restrict__ rec,
-               typename Tr<Real>::Pv* __restrict__ pv) {
+               typename Tr<Real>::Pv* __restrict__ pv, int* __restrict__ order_out = nullptr) {
   using R2 = typename Tr<Real>::R2;
   using Pv = typename Tr<Real>::Pv;
   extern __shared__ int hist[];
@@ -308,9 +311,10 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   const int M = C.M;
   const int Mrec = C.Mrec;
   uint2* slot = scr_slot + R.slot_off + (size_t)local * n;
-  R2* out = rec + R.rec_off + (size_t)local * Mrec;
-  Pv* pre = pv + R.pv_off + (size_t)local * (M + 1);
+  R2* out = kOrder ? nullptr : rec + R.rec_off + (size_t)local * Mrec;
+  Pv* pre = kOrder ? nullptr : pv + R.pv_off + (size_t)local * (M + 1);
   double* pre_d = reinterpret_cast<double*>(pre);   // FP64 view during the scan (Pv is 8 bytes)
+  int* ord = kOrder ? order_out + R.rec_off + (size_t)local * n : nullptr;
   constexpr int kB = 4;   // elements per thread in flight in each pass
   const int stride = blockDim.x * kB;
 
@@ -362,6 +366,10 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   //     malformed input can never address outside the curve.
   auto emit = [&](int p, int i) {
     i = min(max(i, 0), n - 1);
+    if constexpr (kOrder) {
+      ord[p] = i;
+      return;
+    }
     const double2 g = vw[i];
     R2 o;
     o.x = (Real)(g.x * g.y);
@@ -421,6 +429,7 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
     }
   }
   __syncthreads();
+  if constexpr (kOrder) return;
   // (5) prefix of v in place over pre[1..M], accumulated in FP64 for both
   //     forms (the FP32 form then stores each prefix as a float-float pair
   //     (hi, lo) in the same 8 bytes): each warp scans a contiguous range
@@ -1545,6 +1554,61 @@ extern "C" int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* d, void* 
     return run_search<float>(ctx, hs.data(), d->n_curves, d->pass, d->skip_point, d->depth_min, d->flags,
                              d->timing, st);
   return fail(ctx, GTLS_E_INVALID, "unknown precision");
+}
+
+extern "C" int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const double* periods, int64_t n_periods,
+                               int32_t* order_out, void* stream) {
+  if (!ctx) return GTLS_E_INVALID;
+  if (!t || n < 1 || n_periods < 0 || (n_periods > 0 && (!periods || !order_out)))
+    return fail(ctx, GTLS_E_INVALID, "bad arguments to gtls_fold_order");
+  if (n_periods == 0) return GTLS_OK;
+  GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CurveDev<double> C;
+  std::memset(&C, 0, sizeof(C));
+  C.t = t;
+  C.periods = periods;
+  C.np = n_periods;
+  C.n = n;
+  C.M = n;
+  C.Mrec = (n + 1) & ~1;
+  C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
+  // chunks of periods sized to the scratch budget (8 bytes of slots per sample and period)
+  const long long per_chunk = std::max<long long>(
+      1, std::min<long long>((long long)(ctx->chunk_budget / (8 * (size_t)n)), (long long)INT32_MAX));
+  std::vector<Run> runs;
+  for (long long p0 = 0; p0 < n_periods; p0 += per_chunk) {
+    Run r;
+    std::memset(&r, 0, sizeof(r));
+    r.count = (int)std::min<long long>(per_chunk, n_periods - p0);
+    r.pidx0 = p0;
+    r.rec_off = p0 * n;   // offset of the run's rows in order_out
+    runs.push_back(r);
+  }
+  size_t total = 0;
+  carve_size<CurveDev<double>>(total, 1);
+  carve_size<Run>(total, runs.size());
+  carve_size<uint2>(total, (size_t)std::min<long long>(per_chunk, n_periods) * n);
+  void* mem = arena(ctx, total);
+  if (!mem) return fail(ctx, GTLS_E_NOMEM, "scratch allocation failed");
+  Carver cv(mem);
+  CurveDev<double>* d_cd = cv.take<CurveDev<double>>(1);
+  Run* d_runs = cv.take<Run>(runs.size());
+  uint2* slots = cv.take<uint2>((size_t)std::min<long long>(per_chunk, n_periods) * n);
+  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_cd, &C, sizeof(C), cudaMemcpyHostToDevice, st));
+  GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_runs, runs.data(), sizeof(Run) * runs.size(), cudaMemcpyHostToDevice, st));
+  const size_t smem = sizeof(int) << C.nb_log2;
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+  for (size_t k = 0; k < runs.size(); ++k) {
+    prepare_kernel<double, true><<<runs[k].count, kPrepThreads, smem, st>>>(d_cd, d_runs + k, 1, slots, nullptr,
+                                                                             nullptr, order_out);
+    ctx->launches += 1;
+    GTLS_TRY_CUDA(ctx, cudaGetLastError());
+  }
+  // the host copies above read C and runs: wait for them before they go out of scope
+  GTLS_TRY_CUDA(ctx, cudaStreamSynchronize(st));
+  return GTLS_OK;
 }
 
 extern "C" int gtls_duration_ranges(gtls_ctx* ctx, const double* periods, int64_t n_periods, float span,

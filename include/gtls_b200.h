@@ -106,6 +106,19 @@ int gtls_period_grid(gtls_ctx* ctx, double a_over_3, double c, int64_t n_points,
 int gtls_duration_ranges(gtls_ctx* ctx, const double* periods, int64_t n_periods, float span,
                          int32_t n_samples, int32_t* wmin, int32_t* wmax, void* stream);
 
+/*
+ * The stable fold ordering of a light curve for each of n_periods trial
+ * periods: order_out[p * n + j] = index of the sample at sorted position j
+ * of period p, sorting by phase = t/P - (int)(t/P) (foldFast,
+ * GPUFun.py:30-41) with ties kept in index order.  Replaces the cupy
+ * argsort of the folded phases (core.py:775-777); gtls_search computes the
+ * same ordering internally.  order_out: device, n_periods * n int32.
+ * Requires t >= 0 and max(t) / min(period) < 2^31 (the fold's int
+ * truncation, as in the reference).  Synchronises the stream.
+ */
+int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const double* periods, int64_t n_periods,
+                    int32_t* order_out, void* stream);
+
 /* Stage times of one gtls_search call, measured with CUDA events on the
  * call's stream (filled only when gtls_search_desc.timing is non-NULL; the
  * call then synchronises the stream before returning). */

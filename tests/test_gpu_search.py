@@ -241,3 +241,26 @@ def test_search_rejects_invalid_arguments_and_stays_usable(cuda):
     c_ref, _ = O.search_periods(O.NumpyBackend(), P, s["t"], s["y"], s["dy"], s["widths"], s["templates"],
                                 s["overshoot"], s["maxd"], 1e-5, 8, 3)
     np.testing.assert_allclose(c.cpu().numpy(), c_ref, rtol=RTOL64)
+
+
+def test_fold_order_is_the_stable_argsort_of_the_phases(cuda):
+    """The fold ordering, bit for bit: np.argsort(phase, kind="stable") of the
+    reference's foldFast phases, including clustered phases (regular cadence,
+    periods near multiples of it) and exact ties (repeated times)."""
+    import torch
+    from gtls_b200 import _lib
+    rng = np.random.default_rng(9)
+    cad = 10.0 / 1440.0
+    cases = [
+        np.sort(rng.uniform(100.0, 400.0, 3000)),                      # random sampling
+        100.0 + np.arange(5000) * cad,                                  # regular cadence
+        np.repeat(100.0 + np.arange(800) * 0.01, 3),                    # exact ties
+    ]
+    for t in cases:
+        P = np.concatenate([np.exp(rng.uniform(np.log(0.5), np.log(50.0), 40)),
+                            cad * np.array([72.0, 144.0, 1000.0]) * (1 + np.array([1e-9, -3e-8, 0.0]))])
+        dev = torch.device("cuda:0")
+        got = _lib.fold_order(torch.from_numpy(t).to(dev), torch.from_numpy(P).to(dev)).cpu().numpy()
+        for i, p in enumerate(P):
+            ref = np.argsort(O.fold_phases(t, p), kind="stable")
+            np.testing.assert_array_equal(got[i], ref, err_msg="period %r" % p)
