@@ -132,6 +132,19 @@ def test_gtls_batch_power_equals_gtls_power(cuda):
         np.testing.assert_array_equal(np.ma.filled(r.chi2, -1.0), np.ma.filled(ref.chi2, -1.0))
 
 
+def test_gtls_batch_full_stats_equal_gtls(cuda):
+    from gtls_b200 import gtls
+    from gtls_b200.batch import gtls_batch
+    curves = _light_curves()[:2]
+    kw = dict(precision="fp64", batch_periods=20, oversampling_factor=2, use_threads=1)
+    res = gtls_batch(curves).power(full_stats=True, **kw)
+    for (t, y), r in zip(curves, res):
+        ref = gtls(t, y, verbose=False).power(**kw)
+        np.testing.assert_array_equal(r.transit_times, ref.transitTimes)
+        for a, b in (("snr", "snr"), ("snr_pink", "snrPink"), ("snr_fit", "snrFit"), ("snr_fit_pink", "snrFitPink")):
+            assert getattr(r, a) == getattr(ref, b) or (np.isnan(getattr(r, a)) and np.isnan(getattr(ref, b)))
+
+
 def test_gtls_batch_fp32_finds_the_fp64_period(cuda):
     from gtls_b200.batch import gtls_batch
     curves = _light_curves()
