@@ -192,7 +192,7 @@ def cpu_reference(t, y, dy, periods, kw, step, batch_hint, budget_s=15.0, seed=0
         main_n += 1
         i += 1
     while time.time() - t_begin < budget_s and all_n < 3:
-        p = order[i + all_n]
+        p = order[(i + all_n) % len(order)]
         sel = unions[p // batch_hint]
         a = time.time()
         rb.noskip_pass(t, y, dy, periods[p], widths[sel], tm[sel], os_[sel], maxd, 1e-5)
