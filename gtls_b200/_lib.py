@@ -94,7 +94,7 @@ class Tuning(ctypes.Structure):
         ("tile_cap_fp32", ctypes.c_int32),
         ("tile_cap_fp64", ctypes.c_int32),
         ("bucket_shift", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("records_global", ctypes.c_int32),
     ]
 
 
@@ -267,11 +267,11 @@ def fold_order(t, periods, device=0):
     return out
 
 
-def set_tuning(tile_cap_fp32=0, tile_cap_fp64=0, bucket_shift=0, device=0):
+def set_tuning(tile_cap_fp32=0, tile_cap_fp64=0, bucket_shift=0, records_global=0, device=0):
     """Launch-shape parameters of the searches on ``device`` (0 = default);
     results do not depend on them."""
     ctx = context(device)
-    t = Tuning(int(tile_cap_fp32), int(tile_cap_fp64), int(bucket_shift), 0)
+    t = Tuning(int(tile_cap_fp32), int(tile_cap_fp64), int(bucket_shift), int(records_global))
     _check(load().gtls_set_tuning(ctx, ctypes.byref(t)), ctx, "gtls_set_tuning")
 
 
@@ -280,7 +280,8 @@ def get_tuning(device=0):
     ctx = context(device)
     t = Tuning()
     _check(load().gtls_get_tuning(ctx, ctypes.byref(t)), ctx, "gtls_get_tuning")
-    return dict(tile_cap_fp32=t.tile_cap_fp32, tile_cap_fp64=t.tile_cap_fp64, bucket_shift=t.bucket_shift)
+    return dict(tile_cap_fp32=t.tile_cap_fp32, tile_cap_fp64=t.tile_cap_fp64, bucket_shift=t.bucket_shift,
+                records_global=t.records_global)
 
 
 def search(curve, periods, tables, depth_min, skip_point, batch, pass_, precision, device=0,

@@ -235,9 +235,11 @@ int gtls_set_tuning(gtls_ctx* ctx, const gtls_tuning* t) {
   if (!cap_ok(t->tile_cap_fp32) || !cap_ok(t->tile_cap_fp64))
     return fail(ctx, GTLS_E_INVALID, "tile caps must be 0 or multiples of 256 in [256, 65536]");
   if (t->bucket_shift < -3 || t->bucket_shift > 0) return fail(ctx, GTLS_E_INVALID, "bucket_shift must be in [-3, 0]");
+  if (t->records_global != 0 && t->records_global != 1) return fail(ctx, GTLS_E_INVALID, "records_global must be 0 or 1");
   ctx->tile_cap_fp32 = t->tile_cap_fp32 ? t->tile_cap_fp32 : 16384;
   ctx->tile_cap_fp64 = t->tile_cap_fp64 ? t->tile_cap_fp64 : 8192;
   ctx->bucket_shift = t->bucket_shift;
+  ctx->records_global = t->records_global;
   return GTLS_OK;
 }
 
@@ -246,7 +248,7 @@ int gtls_get_tuning(const gtls_ctx* ctx, gtls_tuning* t) {
   t->tile_cap_fp32 = ctx->tile_cap_fp32;
   t->tile_cap_fp64 = ctx->tile_cap_fp64;
   t->bucket_shift = ctx->bucket_shift;
-  t->reserved = 0;
+  t->records_global = ctx->records_global;
   return GTLS_OK;
 }
 

@@ -20,6 +20,7 @@ struct gtls_ctx {
   int tile_cap_fp32 = 16384;   // launch-shape tuning (gtls_set_tuning); results do not depend on it
   int tile_cap_fp64 = 8192;
   int bucket_shift = 0;
+  int records_global = 0;      // 1: chi2 reads records from global memory for every curve
 };
 
 namespace gtls {

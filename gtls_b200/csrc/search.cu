@@ -128,6 +128,7 @@ struct CurveDev {
   long long np;
   int n, maxd, M, Mrec, D, max_width, batch, nbatch;
   int tile, ntiles, nb_log2;
+  int global_rec;               // 1: chi2 reads the records from global memory (no shared tile)
   float span;
 };
 
@@ -762,8 +763,11 @@ __host__ __device__ __forceinline__ size_t chi2_smem_bytes(int tile, int maxd, i
 
 // kAllStarts: the instance for the all-starts pass (every skip is 1), which
 // alone carries the unclamped skip-1 path, so that the main-pass instance
-// keeps its register allocation.
-template <typename Real, bool kAllStarts>
+// keeps its register allocation.  kGlobal: the records are read from global
+// memory (through L1/L2) instead of a shared-memory tile, for curves whose
+// longest duration leaves no room for a tile in shared memory (or when the
+// caller asks for it); results are the same either way.
+template <typename Real, bool kAllStarts, bool kGlobal>
 __global__ void __launch_bounds__(kChiThreads, 1)
 chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs,
             const typename Tr<Real>::R2* __restrict__ rec, const typename Tr<Real>::Pv* __restrict__ pv,
@@ -802,7 +806,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   const int* __restrict__ skips = C.skips;
   const int lane = threadIdx.x & 31;
   // per-duration table after the tile: overshoot, (width | skip << 16), template row offset
-  Real* dtab_os = reinterpret_cast<Real*>(smem_raw + chi2_tile_bytes<Real>(C.tile, C.maxd));
+  Real* dtab_os = reinterpret_cast<Real*>(smem_raw + (kGlobal ? 0 : chi2_tile_bytes<Real>(C.tile, C.maxd)));
   int* dtab_ws = reinterpret_cast<int*>(dtab_os + D);
   int* dtab_row = dtab_ws + D;
   const R2* __restrict__ trows = C.trows;
@@ -816,7 +820,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   // stage the records [k0, k0 + L) in shared memory with one bulk (TMA) copy;
   // the byte count is rounded up to 16 (the record rows are padded for it)
   const uint32_t tile_bytes = (uint32_t)(((size_t)L * sizeof(R2) + 15) & ~(size_t)15);
-  if (threadIdx.x == 0) {
+  if (!kGlobal && threadIdx.x == 0) {
     mbar_init(&tile_bar, 1);
     mbar_arrive_expect_tx(&tile_bar, tile_bytes);
     bulk_g2s(tile, src, tile_bytes, &tile_bar);
@@ -849,20 +853,27 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     if (lane == 0) {
       task_pre[ucnt] = carry;
       task_next = 0;
-      tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
-      if (!tile_ok) atomicOr(a.status, 1);
+      if constexpr (kGlobal) {
+        tile_ok = 1;
+      } else {
+        tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
+        if (!tile_ok) atomicOr(a.status, 1);
+      }
     }
   }
   __syncthreads();
-  // zero the pad after the tile's L records (the copy's rounding to 16 bytes
-  // may have brought in one record past them, possibly an unwritten one)
-  for (int i = L + (int)threadIdx.x; i < L + kTilePad; i += blockDim.x) {
-    R2 zr;
-    zr.x = (Real)0;
-    zr.y = (Real)0;
-    tile[i] = zr;
+  if constexpr (!kGlobal) {
+    // zero the pad after the tile's L records (the copy's rounding to 16 bytes
+    // may have brought in one record past them, possibly an unwritten one)
+    for (int i = L + (int)threadIdx.x; i < L + kTilePad; i += blockDim.x) {
+      R2 zr;
+      zr.x = (Real)0;
+      zr.y = (Real)0;
+      tile[i] = zr;
+    }
   }
   __syncthreads();
+  const R2* recs = kGlobal ? src : tile;   // the records [k0, k0 + L)
 
   Best best{INFINITY, 0x7fffffffffffffffLL};
   // the first start skipped by k % skip != 0 carries the value n (GPUFun.py:407,409)
@@ -910,10 +921,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       const int Qr = (Q + kR - 1) / kR * kR;
       if ((jb + Qr + kR - 1) * s - k0 <= L) {
         for (int rho = lane; rho < s; rho += 32)
-          correlate_pre<Real, kTwoLevel, false>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+          correlate_pre<Real, kTwoLevel, false>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
       } else {
         for (int rho = lane; rho < s; rho += 32)
-          correlate_pre<Real, kTwoLevel, true>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+          correlate_pre<Real, kTwoLevel, true>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
       }
       const Real mine = warp_reduce_scatter18<Real>(acc);
       // lane kLaneOf[r] holds B_r, lane kLaneOf[kR + r] holds C_r
@@ -935,11 +946,11 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       const int jb = jlo + (sub * 32 + lane) * kR;
       if (jb < jhi) {
         const int Qr = (Q + kR - 1) / kR * kR;
-        if (kAllStarts && s == 1 && jb + kR <= jhi) {
-          correlate_s1<Real, kTwoLevel>(tile, jb - k0, trow, Qr, acc);
+        if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
+          correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
         } else {
           for (int rho = 0; rho < s; ++rho)
-            correlate<Real, kTwoLevel>(tile, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+            correlate<Real, kTwoLevel>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
         // the prefix values of the lane's kR starts, all loads in flight
         // together (indices clamped to the last start of the tile; values of
@@ -1184,9 +1195,13 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     }
     if (maxd > 0xffff) return fail(ctx, GTLS_E_RANGE, "max_width above 65535");
     const size_t table = (size_t)D * (sizeof(Real) + 2 * sizeof(int)) + 16;
+    const long long cap = sizeof(Real) == 4 ? ctx->tile_cap_fp32 : ctx->tile_cap_fp64;
     long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd - kTilePad) / 256 * 256;
-    if (tile < 256) return fail(ctx, GTLS_E_RANGE, "light curve too long for the shared-memory tile");
-    tile = std::min<long long>(tile, sizeof(Real) == 4 ? ctx->tile_cap_fp32 : ctx->tile_cap_fp64);
+    // records in global memory when the longest duration leaves no room for a
+    // shared-memory tile of at least 256 starts (or when the caller asks for it)
+    const bool global_rec = ctx->records_global || tile < 256;
+    if (global_rec) tile = cap;
+    tile = std::min<long long>(tile, cap);
     if (tile > n) tile = (n + 255) / 256 * 256;
     C.t = h.t;
     C.y = h.y;
@@ -1209,6 +1224,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     C.tile = (int)tile;
     C.ntiles = (int)((n + tile - 1) / tile);
     C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
+    C.global_rec = global_rec ? 1 : 0;
     C.span = h.span;
     p_off[c + 1] = p_off[c] + h.np;
     b_off[c + 1] = b_off[c] + C.nbatch;
@@ -1230,14 +1246,17 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   std::vector<Run> runs;
   std::vector<int> chunk_r0, chunk_items, chunk_tiles;
   std::vector<size_t> chunk_smem_prep, chunk_smem_chi;
+  std::vector<int> chunk_global;   // per chunk: records of all its curves in global memory (1) or tiles (0)
   size_t max_slot = 0, max_rec = 0, max_pv = 0, max_part = 0;
   {
     size_t slot = 0, rec = 0, pvs = 0, bytes = 0;
     int items = 0, tiles = 0;
     size_t sm_prep = 0, sm_chi = 0;
+    int mode = -1;
     chunk_r0.push_back(0);
     auto close_chunk = [&]() {
       if (items == 0) return;
+      chunk_global.push_back(mode);
       chunk_items.push_back(items);
       chunk_tiles.push_back(tiles);
       chunk_smem_prep.push_back(sm_prep);
@@ -1250,12 +1269,14 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
       slot = rec = pvs = bytes = 0;
       items = tiles = 0;
       sm_prep = sm_chi = 0;
+      mode = -1;
     };
     for (int c = 0; c < n_curves; ++c) {
       const CurveDev<Real>& C = cd[c];
       const size_t per = (size_t)C.n * 8 + (size_t)C.Mrec * sizeof(R2) + (size_t)(C.M + 1) * sizeof(Pv) +
                          (size_t)C.ntiles * 16;
       long long p = 0;
+      if (C.np > 0 && mode != -1 && mode != C.global_rec) close_chunk();   // one records mode per chunk
       while (p < C.np) {
         long long fit = (long long)((budget > bytes ? budget - bytes : 0) / per);
         fit = std::min<long long>(fit, (long long)INT32_MAX - items);
@@ -1284,7 +1305,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
         items += (int)take;
         tiles += (int)(take * C.ntiles);
         sm_prep = std::max(sm_prep, sizeof(int) << C.nb_log2);
-        sm_chi = std::max(sm_chi, chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
+        sm_chi = std::max(sm_chi, C.global_rec ? (size_t)C.D * (sizeof(Real) + 2 * sizeof(int))
+                                               : chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
+        mode = C.global_rec;
         p += take;
       }
     }
@@ -1382,10 +1405,14 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   }
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)std::max<size_t>(max_prep, 1)));
-  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)std::max<size_t>(max_chi, 1)));
-  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)std::max<size_t>(max_chi, 1)));
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, false, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(max_chi, 1)));
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, true, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(max_chi, 1)));
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, false, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(max_chi, 1)));
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, true, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(max_chi, 1)));
   Chi2Args ca;
   ca.pass = precision_pass;
   ca.depth_min = depth_min;
@@ -1403,10 +1430,11 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
     ca.nruns = nr;
-    if (all)
-      chi2_kernel<Real, true><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
-    else
-      chi2_kernel<Real, false><<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
+    using ChiKernel = void (*)(const CurveDev<Real>*, const Run*, const R2*, const Pv*, Chi2Args);
+    const ChiKernel kern = all ? (chunk_global[k] ? &chi2_kernel<Real, true, true> : &chi2_kernel<Real, true, false>)
+                               : (chunk_global[k] ? &chi2_kernel<Real, false, true>
+                                                  : &chi2_kernel<Real, false, false>);
+    kern<<<tiles, kChiThreads, chunk_smem_chi[k], st>>>(d_cd, d_runs + r0, rec, pv, ca);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[2], st));
     finish_kernel<Real><<<(items + 127) / 128, 128, 0, st>>>(d_cd, d_runs + r0, nr, items, part_v, part_loc);
     if (tm) {

@@ -79,7 +79,9 @@ typedef struct gtls_tuning {
   int32_t tile_cap_fp64;      /* the same for the FP64 form, 0 = 8192                        */
   int32_t bucket_shift;       /* phase buckets of the fold ordering = 2^min(15, ceil(log2 N) + shift),
                                  shift in [-3, 0] (0 = default)                               */
-  int32_t reserved;           /* 0                                                            */
+  int32_t records_global;     /* 1: the chi2 kernel reads the folded records from global memory
+                                 (L1/L2) for every curve; 0: from a shared-memory tile when the
+                                 curve's longest duration leaves room for one (default)        */
 } gtls_tuning;
 
 int gtls_set_tuning(gtls_ctx* ctx, const gtls_tuning* tuning);
