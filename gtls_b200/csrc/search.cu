@@ -670,6 +670,63 @@ __device__ __forceinline__ void correlate_pre(const typename Tr<Real>::R2* __res
   }
 }
 
+// correlate_pre() over all of a lane's offsets rho = lane, lane + 32, ... < s
+// for a task whose template rows fit one block (Q <= kR) and whose reads stay
+// in the tile, with the accumulators carried from one rho to the next (the
+// single-level form).  One rho's 2*kR-1 record steps update 1, 2, ..., kR,
+// ..., 2, 1 accumulators; here the last kR-1 steps of one rho run together
+// with the first kR-1 of the next, so that every step updates each of the kR
+// accumulators exactly once (no short dependency chains at the ends of a
+// rho).  Each accumulator still receives its products in the same order
+// (rho by rho, and within a rho by record), so the sums are bitwise those of
+// correlate_pre().  Template slot q switches to the next rho at step q: its
+// last use for the previous rho is at step q - 1.
+template <typename Real>
+__device__ __forceinline__ void correlate_rounds(const typename Tr<Real>::R2* __restrict__ tile, int base, int s,
+                                                 const typename Tr<Real>::R2* __restrict__ trow, int lane,
+                                                 typename Tr<Real>::R2 (&acc)[kR]) {
+  using R2 = typename Tr<Real>::R2;
+  const int nr = (s - lane + 31) >> 5;   // offsets of this lane (s >= 32, so at least one)
+  const R2* xh = tile + base + lane;     // records of the current rho: x[m] = xh[m * s]
+  const R2* th = trow + lane;            // its template entries: t[q] = th[q * s]
+  R2 tq[kR];
+#pragma unroll
+  for (int q = 0; q < kR; ++q) tq[q] = th[q * s];
+  // first rho: its first kR steps (step m updates r = 0..m)
+#pragma unroll
+  for (int m = 0; m < kR; ++m) {
+    const R2 x = xh[m * s];
+#pragma unroll
+    for (int r = m; r >= 0; --r) fma_pair(tq[m - r], x, acc[r]);
+  }
+  for (int i = 1; i < nr; ++i) {
+    const R2* xt = xh;
+    xh += 32;
+    th += 32;
+    // step m: the previous rho's step kR + m (r = m+1..kR-1, template slots
+    // m+1..kR-1 still hold its entries), then this rho's step m (r = m..0)
+#pragma unroll
+    for (int m = 0; m < kR; ++m) {
+      tq[m] = th[m * s];
+      if (m < kR - 1) {
+        const R2 xa = xt[(kR + m) * s];
+#pragma unroll
+        for (int r = kR - 1; r > m; --r) fma_pair(tq[kR + m - r], xa, acc[r]);
+      }
+      const R2 xb = xh[m * s];
+#pragma unroll
+      for (int r = m; r >= 0; --r) fma_pair(tq[m - r], xb, acc[r]);
+    }
+  }
+  // last rho: its remaining kR-1 steps
+#pragma unroll
+  for (int m = 0; m < kR - 1; ++m) {
+    const R2 xa = xh[(kR + m) * s];
+#pragma unroll
+    for (int r = kR - 1; r > m; --r) fma_pair(tq[kR + m - r], xa, acc[r]);
+  }
+}
+
 // Butterfly reduce-scatter of 2*kR = 18 per-lane values over the warp
 // (9 + 5 + 3 + 2 + 1 shuffles): value i ends, summed over all lanes, in lane
 // kLaneOf[i].  Returns this lane's value (meaningful only in those lanes).
@@ -920,8 +977,12 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       // every load of the task inside the tile: no clamping needed
       const int Qr = (Q + kR - 1) / kR * kR;
       if ((jb + Qr + kR - 1) * s - k0 <= L) {
-        for (int rho = lane; rho < s; rho += 32)
-          correlate_pre<Real, kTwoLevel, false>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+        if (!kTwoLevel && Qr == kR) {
+          correlate_rounds<Real>(recs, jb * s - k0, s, trow, lane, acc);
+        } else {
+          for (int rho = lane; rho < s; rho += 32)
+            correlate_pre<Real, kTwoLevel, false>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+        }
       } else {
         for (int rho = lane; rho < s; rho += 32)
           correlate_pre<Real, kTwoLevel, true>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
