@@ -711,9 +711,9 @@ def main():
     from gtls_b200 import tune
     tuning = fixed_or_tuned(args, lambda: tune.tune_curve(cur, periods, args.precision), device)
 
-    def one_step(timing=None):
+    def one_step(timing=None, phases=None):
         return core.run_search(cur, periods, periods_dev, t, y, dy, 1e-5, 0.125, kw["oversampling_factor"],
-                               precision=args.precision, batch_periods=batch, timing=timing)
+                               precision=args.precision, batch_periods=batch, timing=timing, phases=phases)
 
     for _ in range(args.warmup):
         one_step()
@@ -739,6 +739,10 @@ def main():
             step_ms.append(e0.elapsed_time(e1))
             timings.append(tm.as_dict())
     launches = _lib.launch_count(device) - launches0
+    # where one search's time goes: one more (untimed) step with a device
+    # synchronisation at each phase boundary
+    phases = {}
+    one_step(phases=phases)
     total_ms = sum(step_ms)
     if world > 1:
         tt = torch.tensor([total_ms], dtype=torch.float64, device=cur.dev)
@@ -816,6 +820,8 @@ def main():
                  "flops": "2 per (start, template sample) for B and for C"},
         "stages_ms": {k: statistics.mean(tm[k] for tm in timings) for k in
                       ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
+        "phases_ms": {"what": "one extra untimed search, wall clock per phase with a device synchronisation at "
+                              "each boundary", **{k: 1000.0 * v for k, v in phases.items()}},
         "result": {"period": float(out[1]), "true_period": truth["period"], "SDE": float(out[7])},
         "trial_evaluations": {
             "what": "(period, duration, start) chi2 evaluations of the main pass per step (the re-searches come on top)",

@@ -131,30 +131,6 @@ def prepare_curve(t, y, dy, opts, device=0):
                 durations=durs, tmpl=tmpl, maxd=int(maxd), duration_grid=np.asarray(durations))
 
 
-class _Phases:
-    """Wall-clock time per phase of a batched search (a dict given by the
-    caller), with a device synchronisation at each boundary; no-op when the
-    caller gives none."""
-
-    def __init__(self, out):
-        self.out = out
-        self.t = None
-        if out is not None:
-            import time
-            import torch
-            self._time, self._sync = time.perf_counter, torch.cuda.synchronize
-            self._sync()
-            self.t = self._time()
-
-    def mark(self, name):
-        if self.out is None:
-            return
-        self._sync()
-        now = self._time()
-        self.out[name] = self.out.get(name, 0.0) + (now - self.t)
-        self.t = now
-
-
 def _offsets(counts):
     return np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
 
@@ -200,7 +176,7 @@ class gtls_batch(object):
             if per_curve_batch:
                 sub = types.SimpleNamespace(**vars(opts))
                 sub.batch_periods = np.asarray(opts.batch_periods)[list(indices)]
-            ph = _Phases(phases)
+            ph = core.Phases(phases)
             prepared = [prepare_curve(*self.curves[i], sub, device=device) for i in indices]
             ph.mark("prepare_curves")
             return search_prepared(prepared, sub, device=device, full_stats=full_stats,
@@ -281,7 +257,7 @@ def search_prepared(prepared, opts, device=0, full_stats=False, keep_spectra=Tru
     ``keep_spectra``) periods, power and chi2 as masked arrays.  With
     ``autotune`` the launch shapes are first tuned on the set's largest
     curve (``tune.tune_curve_set``; cached per shape, results unchanged)."""
-    ph = _Phases(phases)
+    ph = core.Phases(phases)
     cs = CurveSetOnDevice(prepared, device=device)
     ph.mark("upload")
     if autotune:
@@ -295,7 +271,7 @@ def search_on_device(cs, opts, full_stats=False, keep_spectra=True, timing=None,
     """The batched search of a ``CurveSetOnDevice`` (see ``search_prepared``).
     ``phases``: optional dict receiving the wall-clock seconds of each phase."""
     import torch
-    ph = _Phases(phases)
+    ph = core.Phases(phases)
     prepared = cs.prepared
     device = cs.device
     dev = cs.dev

@@ -42,6 +42,30 @@ def reference_batch_size(n_periods, n_samples, maxd, n_durations, free_bytes):
     return max(1, s)
 
 
+class Phases:
+    """Wall-clock time per phase of a search (a dict given by the caller),
+    with a device synchronisation at each boundary; no-op when the caller
+    gives none."""
+
+    def __init__(self, out):
+        self.out = out
+        self.t = None
+        if out is not None:
+            import time
+            import torch
+            self._time, self._sync = time.perf_counter, torch.cuda.synchronize
+            self._sync()
+            self.t = self._time()
+
+    def mark(self, name):
+        if self.out is None:
+            return
+        self._sync()
+        now = self._time()
+        self.out[name] = self.out.get(name, 0.0) + (now - self.t)
+        self.t = now
+
+
 def find_nearest_indices(a, b):
     """Nearest element of ``b`` to each value of ``a``, first occurrence (core.py:34-46)."""
     a = np.asarray(a, dtype=float)
@@ -186,7 +210,8 @@ def search_multi_periods(periods, t, y, dy, transit_depth_min, lc_arr, lc_cache_
 
 
 def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_margin, oversampling_factor,
-               fast=False, precision="fp64", batch_periods=None, timing=None, distributed=False, group=None):
+               fast=False, precision="fp64", batch_periods=None, timing=None, distributed=False, group=None,
+               phases=None):
     """The search on a curve already resident on the device (see search_multi_periods).
 
     ``periods``: sorted host array, ``periods_dev`` the same on the device.
@@ -194,9 +219,12 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     ``distributed``: shard the main pass over the ranks of the initialised
     process group ``group`` (batch-aligned period ranges, chi2 all-gathered);
     every rank then finishes the search and returns the same result.
+    ``phases``: optional dict receiving the wall-clock seconds of each phase
+    (a device synchronisation at each boundary).
     """
     import torch
     from . import shard
+    ph = Phases(phases)
     device = cur.device
     skip = skip_point_of(T0_fit_margin)
     rank, world = shard.world_info(group) if distributed else (0, 1)
@@ -226,6 +254,7 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     else:
         chi2_dev, _ = cur.search(periods_dev, transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision,
                                  timing=timing)
+    ph.mark("main_pass")
     raw_chi2 = _d2h(chi2_dev)
     median = np.median(raw_chi2)
     mask = raw_chi2 > (100 * median)
@@ -233,6 +262,7 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
     raw_power = ma.array(_d2h(power_dev), mask=mask)
     mperiods = ma.array(periods, mask=mask)
+    ph.mark("spectra")
     if fast:
         return mperiods, raw_power
 
@@ -241,12 +271,15 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     cand_idx = _candidates(power_dev, mask_dev, periods_dev, torch)
     TRANSFER["d2h"] += cand_idx.nbytes
     cand_p = periods[cand_idx]
+    ph.mark("candidates")
     again, _ = cur.search(cand_p, transit_depth_min, skip, S, _lib.GTLS_PASS_ALL,
                           "fp32" if precision == "fp32" else "fp64")
+    ph.mark("candidate_search")
     ci = _h2d(torch, cand_idx, dev)
     chi2_dev[ci] = again
     mask_dev[ci] = 0
     _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
+    ph.mark("spectra")
     rechecked = np.zeros(0, dtype=np.int64)
     if precision == "fp32":
         def search64(p, union):
@@ -260,6 +293,7 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
             _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
         rechecked = cand_idx[pos]
         again = chi2_dev[ci]
+        ph.mark("fp64_recheck")
     pw = power_dev[ci]
     best = int(cand_idx[int(torch.argmax(pw).item())])
     period = periods[best]
@@ -273,8 +307,9 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     _, _, power_dev, sde_raw, sde = _spectra(chi2_dev, mask_dev, oversampling_factor, device)
     best = int(h_idx[int(torch.argmax(power_dev[hi]).item())])
     period = float(periods[best])
+    ph.mark("harmonics")
 
-    fin = single_period(cur, period, t, y, dy, transit_depth_min)
+    fin = single_period(cur, period, t, y, dy, transit_depth_min, phases=ph)
 
     chi2_h = _d2h(chi2_dev)
     # core.py:892-895 wraps raw_chi2 in a masked array without copying, so the
@@ -287,6 +322,7 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
     chi2_m = ma.array(chi2_h, mask=mask_h)
     power_m = ma.array(power_h, mask=mask_h)
     periods_m = ma.array(periods, mask=mask_h)
+    ph.mark("outputs")
     diag = dict(batch_periods=S, period_index=best, sde_raw=sde_raw, again=_d2h(again), chi2_main=chi2_main,
                 fp64_rechecked=rechecked,
                 harmonic_indices=h_idx, chi2_harmonics=_d2h(again2), loc=fin["loc"],
@@ -296,14 +332,19 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
             fin["snr_fit_pink"], raw_power, raw_chi2, list(cand_idx), list(cand_p), diag)
 
 
-def single_period(cur, period, t, y, dy, transit_depth_min):
+def single_period(cur, period, t, y, dy, transit_depth_min, phases=None):
     """core.search_single_periods (core.py:1250-1505): chi2 over the period's own
-    duration range at every start on the GPU, then the host statistics."""
+    duration range at every start on the GPU, then the host statistics.
+    ``phases``: optional ``Phases`` marking the two parts."""
     chi2, loc = cur.search(np.array([period]), transit_depth_min, 1, 1, _lib.GTLS_PASS_ALL, "fp64",
                            want_loc=True)
     loc = int(_d2h(loc)[0])
+    if phases is not None:
+        phases.mark("best_period_search")
     fin = finish_period(cur.widths, cur.durations, cur.overshoot, cur.maxd, cur.curve["span"], period, loc, t, y,
                         device=cur.device)
+    if phases is not None:
+        phases.mark("best_period_stats")
     fin["chi2"] = float(_d2h(chi2)[0])
     return fin
 

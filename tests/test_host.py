@@ -119,3 +119,22 @@ def test_fp64_recheck_plan_uses_each_batch_union(monkeypatch):
         assert np.all(sel // S == g)
         np.testing.assert_array_equal(union, np.nonzero(valid[g * S:(g + 1) * S].any(axis=0))[0])
     assert 7 not in chosen
+
+
+def test_phases_accumulate_per_name(monkeypatch):
+    """core.Phases: wall-clock seconds per phase name, summed over repeated
+    marks; a no-op without a dict (no device synchronisation either)."""
+    import torch
+    from gtls_b200.core import Phases
+    calls = []
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a: calls.append(1))
+    out = {}
+    ph = Phases(out)
+    ph.mark("a")
+    ph.mark("b")
+    ph.mark("a")
+    assert set(out) == {"a", "b"} and all(v >= 0.0 for v in out.values())
+    assert len(calls) == 4
+    calls.clear()
+    Phases(None).mark("x")
+    assert calls == []
