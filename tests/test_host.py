@@ -138,3 +138,52 @@ def test_phases_accumulate_per_name(monkeypatch):
     calls.clear()
     Phases(None).mark("x")
     assert calls == []
+
+
+def _transit_fluxes_by_mask(t, y, mids, dur):
+    out = []
+    for mid in mids:
+        a, b = mid - 0.5 * dur, mid + 0.5 * dur
+        out.append(None if np.isnan(a) or np.isnan(b) else y[np.logical_and(t > a, t < b)])
+    return out
+
+
+def test_transit_fluxes_equal_the_mask():
+    """stats._transit_fluxes (binary search on sorted times) selects the
+    samples the reference's per-transit mask selects, in the same order,
+    including bounds that fall exactly on sample times, repeated times,
+    transits outside the data, NaN mid-times and unsorted times."""
+    from gtls_b200 import stats
+    rng = np.random.default_rng(5)
+    t = np.sort(rng.uniform(0.0, 30.0, 4000))
+    t[100:110] = t[100]                                   # repeated times
+    y = rng.normal(1.0, 1e-3, len(t))
+    dur = 0.125
+    mids = list(np.arange(-1.0, 32.0, 0.7)) + [t[500] + 0.5 * dur, t[900] - 0.5 * dur, np.nan, t[100]]
+    for tt in (t, t[rng.permutation(len(t))]):
+        yy = y if tt is t else y[np.argsort(np.argsort(tt))]
+        got = stats._transit_fluxes(tt, yy, mids, dur)
+        want = _transit_fluxes_by_mask(tt, yy, mids, dur)
+        assert len(got) == len(want)
+        for g, w in zip(got, want):
+            assert (g is None) == (w is None)
+            if g is not None:
+                np.testing.assert_array_equal(g, w)
+
+
+def test_pink_noise_matches_per_window_std():
+    import pytest
+    """stats.pink_noise (prefix sums in extended precision) against the
+    reference's loop over windows (stats.py:426-431: the mean over windows of
+    np.std(window) / sqrt(width)), within 1e-12 relative."""
+    from gtls_b200 import stats
+    rng = np.random.default_rng(9)
+    x = 1.0 + rng.normal(0.0, 1e-3, 5000)
+    x[1000:1040] -= 2e-3                                  # a transit-like dip
+    for data, width in ((x, 1), (x, 2), (x, 15), (x, 300), (x[:40], 40), (x[:3] * 0 + 1.0, 2)):
+        n = len(data) - width + 1
+        ref = sum(np.std(data[i:i + width]) / width ** 0.5 for i in range(n)) / n
+        got = stats.pink_noise(data, width)
+        assert abs(got - ref) <= 1e-12 * abs(ref) + 1e-300, (width, got, ref)
+    with pytest.raises(ValueError):
+        stats.pink_noise(x[:5], 6)
