@@ -1302,6 +1302,29 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     rows_total += rows;
   }
 
+  // ---- small searches (a few periods: the harmonics, the best period):
+  // narrower tiles, so that the chi2 launch still has about two CTAs per SM
+  // (a start's value does not depend on the width of its tile)
+  {
+    long long ctas = 0, np_total = 0;
+    for (int c = 0; c < n_curves; ++c) {
+      ctas += cd[c].np * cd[c].ntiles;
+      np_total += cd[c].np;
+    }
+    const long long want = 2LL * ctx->num_sms;
+    if (np_total > 0 && ctas < want) {
+      const long long per = (want + np_total - 1) / np_total;   // tiles wanted per period
+      for (int c = 0; c < n_curves; ++c) {
+        CurveDev<Real>& C = cd[c];
+        const long long narrow = std::max<long long>(256, ((C.n + per - 1) / per + 255) / 256 * 256);
+        if (narrow < C.tile) {
+          C.tile = (int)narrow;
+          C.ntiles = (int)((C.n + narrow - 1) / narrow);
+        }
+      }
+    }
+  }
+
   // ---- chunks of the period list (curve after curve) and their runs
   const size_t budget = ctx->chunk_budget;
   std::vector<Run> runs;
