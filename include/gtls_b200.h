@@ -7,7 +7,11 @@
  * where it says it synchronises.  Every call returns 0 on success and a
  * GTLS_E_* code otherwise; gtls_last_error() gives the message.  No C++
  * exception crosses this interface.  A context belongs to one device and
- * must not be used from two host threads at once.
+ * must not be used from two host threads at once.  Its calls share one
+ * scratch arena: calls on one context that go to different streams must be
+ * ordered by the caller (an event or a synchronisation between them); calls
+ * on one stream are ordered by the stream.  Use one context per concurrent
+ * stream for overlapping searches.
  *
  * These entry points replace the reference's cupy RawModule kernel launches
  * and their host glue (reference file:line given per function).
