@@ -1628,6 +1628,11 @@ extern "C" int gtls_search_batch(gtls_ctx* ctx, const gtls_batch_desc* d, void* 
   if (d->n_curves < 1 || !d->sample_off || !d->period_off || !d->dur_off || !d->tmpl_off || !d->max_width ||
       !d->batch || !d->span)
     return fail(ctx, GTLS_E_INVALID, "null host array or no curves");
+  // device bases first: a NULL base plus a curve's offset would not be NULL
+  const bool any_period = d->period_off[d->n_curves] != d->period_off[0];
+  if (!d->t || !d->y || !d->dy || !d->widths || !d->overshoot || !d->templates ||
+      (any_period && (!d->periods || !d->chi2_out)))
+    return fail(ctx, GTLS_E_INVALID, "null device array");
   if (d->skip_point < 1) return fail(ctx, GTLS_E_INVALID, "skip_point must be >= 1");
   if (d->pass != GTLS_PASS_MAIN && d->pass != GTLS_PASS_ALL) return fail(ctx, GTLS_E_INVALID, "unknown pass");
   if (d->flags & ~GTLS_SEARCH_ALL_DURATIONS) return fail(ctx, GTLS_E_INVALID, "unknown flags");
