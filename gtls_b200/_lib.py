@@ -208,8 +208,20 @@ def _torch():
     return torch
 
 
+_last_stream = {}
+
+
 def _stream(torch, device):
-    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    """The current stream of ``device`` for the next call, as a void*.  A
+    device's calls share its context's scratch arena, so when the stream
+    differs from the one of the previous call on the device, the new stream
+    first waits for the old one."""
+    cur = torch.cuda.current_stream(device)
+    prev = _last_stream.get(device)
+    if prev is not None and prev != cur:
+        cur.wait_stream(prev)
+    _last_stream[device] = cur
+    return ctypes.c_void_p(cur.cuda_stream)
 
 
 def _ptr(t):

@@ -187,3 +187,40 @@ def test_pink_noise_matches_per_window_std():
         assert abs(got - ref) <= 1e-12 * abs(ref) + 1e-300, (width, got, ref)
     with pytest.raises(ValueError):
         stats.pink_noise(x[:5], 6)
+
+
+def test_calls_on_a_new_stream_wait_for_the_previous_one():
+    """_lib._stream: a device's calls share one scratch arena, so a call on a
+    different stream than the device's previous call first makes its stream
+    wait for the previous one (no wait while the stream stays the same)."""
+    import types
+    from gtls_b200 import _lib
+
+    class FakeStream:
+        def __init__(self, h):
+            self.cuda_stream = h
+            self.waited = []
+
+        def __eq__(self, other):
+            return self.cuda_stream == other.cuda_stream
+
+        def __ne__(self, other):
+            return not self == other
+
+        def wait_stream(self, other):
+            self.waited.append(other.cuda_stream)
+
+    a, b = FakeStream(11), FakeStream(22)
+    current = {"s": a}
+    fake = types.SimpleNamespace(cuda=types.SimpleNamespace(current_stream=lambda device: current["s"]))
+    saved = dict(_lib._last_stream)
+    try:
+        _lib._last_stream.clear()
+        assert _lib._stream(fake, 5).value == 11 and a.waited == []
+        assert _lib._stream(fake, 5).value == 11 and a.waited == []
+        current["s"] = b
+        assert _lib._stream(fake, 5).value == 22 and b.waited == [11]
+        assert _lib._stream(fake, 6).value == 22 and b.waited == [11]      # other device: independent
+    finally:
+        _lib._last_stream.clear()
+        _lib._last_stream.update(saved)
