@@ -24,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -111,12 +112,15 @@ def workload(name, rank=0):
 
 
 class Clocks:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling during the timed region.  The raw
+    samples go to GTLS_CLOCKS_DIR (default: the system temporary directory);
+    the JSON line carries their summary."""
 
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+        out = os.environ.get("GTLS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, "clocks_%d.csv" % os.getpid())
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)

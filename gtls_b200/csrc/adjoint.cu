@@ -1,7 +1,7 @@
 // Chi2 of an unfolded limb-darkened transit model and its adjoint (gradient
 // with respect to the six shape parameters), for many light curves at once.
-// No counterpart in the reference (north-star addition): it refines a
-// search peak below the period/duration grid resolution.
+// An addition with no counterpart in the reference: it refines a search
+// peak below the period/duration grid resolution.
 //
 // Model, for one light curve with parameters (P, T0, D, depth, u1, u2):
 //   n    = round((t - T0) / P)                 nearest transit epoch

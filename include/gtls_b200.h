@@ -252,8 +252,8 @@ int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t
  * Chi2 of the unfolded limb-darkened transit model and its gradient, for
  * n_curves light curves concatenated in t/y/w (curve c owns samples
  * curve_off[c] .. curve_off[c+1]-1, w = 1/dy^2).  params[6c..6c+5] =
- * (P, T0, D, depth, u1, u2) of curve c.  No counterpart in the reference
- * (north-star addition used to refine a search peak below grid resolution).
+ * (P, T0, D, depth, u1, u2) of curve c.  An addition with no counterpart in
+ * the reference, used to refine a search peak below grid resolution.
  * Model: tau = (t-T0) - P round((t-T0)/P), s = 2 tau / D,
  * m = 1 - depth B(s) I(s) / I(0), B = sigmoid((1-s^2)/0.05),
  * I = 1 - u1 (1-mu) - u2 (1-mu)^2, mu = sqrt(max(softplus_200(1-s^2), 1e-300)).
