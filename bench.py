@@ -119,8 +119,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        out = os.environ.get("GTLS_CLOCKS_DIR") or tempfile.gettempdir()
-        self.path = os.path.join(out, "clocks_%d.csv" % os.getpid())
+        out = os.environ.get("GTLS_CLOCKS_DIR")
+        self.keep = bool(out)
+        self.path = os.path.join(out or tempfile.gettempdir(), "clocks_%d.csv" % os.getpid())
+        self._summary = None
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -143,6 +145,13 @@ class Clocks:
             self.proc.wait()
 
     def summary(self):
+        if self._summary is None:
+            self._summary = self._read()
+            if not self.keep and os.path.exists(self.path):
+                os.remove(self.path)
+        return self._summary
+
+    def _read(self):
         if self.proc is None or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()

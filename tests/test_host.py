@@ -224,3 +224,31 @@ def test_calls_on_a_new_stream_wait_for_the_previous_one():
     finally:
         _lib._last_stream.clear()
         _lib._last_stream.update(saved)
+
+
+def test_bench_clock_summary_reads_throttle_reasons(tmp_path, monkeypatch):
+    """bench.Clocks: median SM clock, max clock and the active throttle
+    reasons from nvidia-smi's CSV samples; the raw file is kept only when
+    GTLS_CLOCKS_DIR names a folder for it."""
+    import os
+    import sys
+    from conftest import ROOT
+    sys.path.insert(0, ROOT)
+    import bench
+    rows = ["0, 1965, 1965, 900.0, 0x0, Not Active, Not Active, Not Active, Active",
+            "0, 1900, 1965, 990.0, 0x0, Not Active, Not Active, Not Active, Active",
+            "0, 1965, 1965, 950.0, 0x0, Not Active, Not Active, Not Active, Not Active"]
+    for keep in (False, True):
+        if keep:
+            monkeypatch.setenv("GTLS_CLOCKS_DIR", str(tmp_path))
+        else:
+            monkeypatch.delenv("GTLS_CLOCKS_DIR", raising=False)
+        c = bench.Clocks(0)
+        c.proc = object()                     # as if nvidia-smi had been started
+        with open(c.path, "w") as f:
+            f.write("\n".join(rows) + "\n")
+        s = c.summary()
+        assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
+        assert s["reasons"] == ["sw_power_cap"]
+        assert os.path.exists(c.path) == keep
+        assert c.summary() == s
