@@ -90,9 +90,31 @@ def fractional_transit(duration, maxwidth, depth, samples, reference_flux):
     return 1 - ((1 - result) * depth)
 
 
+def _linspaces(counts):
+    """``np.linspace(-0.5, 0.5, k)`` for every k of ``counts`` (each >= 2),
+    concatenated, with numpy's own arithmetic: index * (1 / (k - 1)), then
+    + (-0.5), and the last point set to 0.5 exactly."""
+    counts = np.asarray(counts, dtype=np.int64)
+    off = np.concatenate(([0], np.cumsum(counts)))
+    seg = np.repeat(np.arange(len(counts)), counts)
+    idx = (np.arange(off[-1]) - off[seg]).astype(float)
+    x = idx * (1.0 / (counts - 1).astype(float))[seg]
+    x += -0.5
+    x[off[1:] - 1] = 0.5
+    return x, off
+
+
 def get_cache(durations, maxwidth_in_samples, per, rp, a, inc, ecc, w, u, limb_dark,
               verbose=True):
-    """Template per duration plus (duration, width_in_samples, overshoot) (transit.py:98-160)."""
+    """Template per duration plus (duration, width_in_samples, overshoot) (transit.py:98-160).
+
+    The in-transit part of fractional_transit(duration, dmax, SIGNAL_DEPTH,
+    samples, ref) for every duration at once: its padding is
+    1 - (1 - 1) * depth = 1 exactly, never below the cutoff, so the trimmed
+    signal comes from the squeezed template alone.  The squeezed templates
+    of all durations are interpolated in one pass (each value computed as
+    the per-duration interpolation computes it)."""
+    durations = np.atleast_1d(np.asarray(durations, dtype=float))
     rows = np.size(durations)
     overview = np.zeros(rows, dtype=[("duration", "f8"), ("width_in_samples", "i8"),
                                      ("overshoot", "f8")])
@@ -101,27 +123,25 @@ def get_cache(durations, maxwidth_in_samples, per, rp, a, inc, ecc, w, u, limb_d
     samples = maxwidth_in_samples
     reference_time = np.linspace(-0.5, 0.5, samples)
     cutoff = 1 - constants.NUMERICAL_STABILITY_CUTOFF
-    lc_arr = []
-    for row, duration in enumerate(durations):
-        # the in-transit part of fractional_transit(duration, dmax, SIGNAL_DEPTH,
-        # samples, ref): its padding is 1 - (1 - 1) * depth = 1 exactly, never
-        # below the cutoff, so the trimmed signal comes from the squeezed
-        # template alone (same values, no padded array built)
-        occupied = int((duration / dmax) * samples)
-        y_new = interp_linear(np.linspace(-0.5, 0.5, occupied), reference_time, ref)
-        scaled = 1 - ((1 - y_new) * constants.SIGNAL_DEPTH)
-        overview["duration"][row] = duration
-        overview["width_in_samples"][row] = int((duration / dmax) * maxwidth_in_samples)
-        full = np.nonzero(scaled < cutoff)[0]
+    occupied = np.array([int((d / dmax) * samples) for d in durations], dtype=np.int64)
+    overview["duration"] = durations
+    overview["width_in_samples"] = [int((d / dmax) * maxwidth_in_samples) for d in durations]
+    if np.all(occupied >= 2):
+        x_new, off = _linspaces(occupied)
+        scaled_all = 1 - ((1 - interp_linear(x_new, reference_time, ref)) * constants.SIGNAL_DEPTH)
+        segments = [scaled_all[off[r]:off[r + 1]] for r in range(rows)]
+    else:
+        segments = [1 - ((1 - interp_linear(np.linspace(-0.5, 0.5, k), reference_time, ref))
+                         * constants.SIGNAL_DEPTH) for k in occupied]
+    lc = np.empty(rows, dtype=object)
+    for row, scaled in enumerate(segments):
+        full = np.flatnonzero(scaled < cutoff)
         if np.size(full) == 0:
             raise ValueError("transit template of duration %g has no in-transit samples "
-                             "(light curve too short for this duration grid)" % duration)
-        signal = scaled[full[0]: full[-1] + 1]
-        lc_arr.append(signal)
+                             "(light curve too short for this duration grid)" % durations[row])
+        signal = scaled[full[0]: full[-1] + 1].copy()
+        lc[row] = signal
         overview["overshoot"][row] = 1 / (2 - np.mean(signal) / np.min(signal))
-    lc = np.empty(len(lc_arr), dtype=object)
-    for i, s in enumerate(lc_arr):
-        lc[i] = s
     return overview, lc
 
 

@@ -172,10 +172,10 @@ def test_transit_fluxes_equal_the_mask():
 
 
 def test_pink_noise_matches_per_window_std():
-    import pytest
     """stats.pink_noise (prefix sums in extended precision) against the
     reference's loop over windows (stats.py:426-431: the mean over windows of
     np.std(window) / sqrt(width)), within 1e-12 relative."""
+    import pytest
     from gtls_b200 import stats
     rng = np.random.default_rng(9)
     x = 1.0 + rng.normal(0.0, 1e-3, 5000)
@@ -252,3 +252,41 @@ def test_bench_clock_summary_reads_throttle_reasons(tmp_path, monkeypatch):
         assert s["reasons"] == ["sw_power_cap"]
         assert os.path.exists(c.path) == keep
         assert c.summary() == s
+
+
+def _get_cache_per_duration(durations, mw, *planet):
+    """The template cache one duration at a time (the reference's loop,
+    transit.py:98-160, with fractional_transit's in-transit part)."""
+    from gtls_b200 import constants
+    ref = template.reference_transit(mw, *planet)
+    dmax = np.max(durations)
+    rt = np.linspace(-0.5, 0.5, mw)
+    widths, overs, lcs = [], [], []
+    for d in durations:
+        occ = int((d / dmax) * mw)
+        sc = 1 - ((1 - template.interp_linear(np.linspace(-0.5, 0.5, occ), rt, ref)) * constants.SIGNAL_DEPTH)
+        full = np.nonzero(sc < 1 - constants.NUMERICAL_STABILITY_CUTOFF)[0]
+        sig = sc[full[0]: full[-1] + 1]
+        widths.append(int((d / dmax) * mw))
+        overs.append(1 / (2 - np.mean(sig) / np.min(sig)))
+        lcs.append(sig)
+    return np.array(widths), np.array(overs), lcs
+
+
+def test_template_cache_equals_the_per_duration_loop():
+    """template.get_cache interpolates all durations in one pass: bitwise the
+    values of the per-duration loop, on random duration grids and widths."""
+    planet = (12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+    rng = np.random.default_rng(4)
+    for _ in range(6):
+        mw = int(rng.integers(200, 6000)) * 2
+        dmin = rng.uniform(0.002, 0.01)
+        durations = dmin * 1.1 ** np.arange(int(rng.integers(5, 45)))
+        ov, lc = template.get_cache(durations, mw, *planet, verbose=False)
+        w_ref, o_ref, lc_ref = _get_cache_per_duration(durations, mw, *planet)
+        np.testing.assert_array_equal(ov["width_in_samples"], w_ref)
+        np.testing.assert_array_equal(ov["overshoot"], o_ref)
+        np.testing.assert_array_equal(ov["duration"], durations)
+        assert len(lc) == len(lc_ref)
+        for a, b in zip(lc, lc_ref):
+            np.testing.assert_array_equal(a, b)
