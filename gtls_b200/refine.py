@@ -45,17 +45,21 @@ def model_chi2_function():
 
 
 def pack_curves(curves, device):
-    """Concatenate [(t, y, dy), ...] into device tensors (t, y, w, off)."""
+    """Concatenate [(t, y, dy), ...] into device tensors (t, y, w, off).
+
+    The weights w = 1 / (dy * dy) are formed on the device from the copied
+    uncertainties (one IEEE multiply and divide: the values the host would
+    compute, without a host pass over every sample)."""
     torch = _torch()
     lens = [len(c[0]) for c in curves]
     off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
     t = np.concatenate([np.asarray(c[0], dtype=np.float64) for c in curves])
     y = np.concatenate([np.asarray(c[1], dtype=np.float64) for c in curves])
     dy = np.concatenate([np.asarray(c[2], dtype=np.float64) for c in curves])
-    w = 1.0 / (dy * dy)
     dev = torch.device(device)
-    return (torch.from_numpy(t).to(dev), torch.from_numpy(y).to(dev), torch.from_numpy(w).to(dev),
-            torch.from_numpy(off).to(dev))
+    dy_d = torch.from_numpy(dy).to(dev)
+    w = 1.0 / (dy_d * dy_d)
+    return torch.from_numpy(t).to(dev), torch.from_numpy(y).to(dev), w, torch.from_numpy(off).to(dev)
 
 
 def refine(params0, scales, t, y, w, off, steps=50, lr=0.05):

@@ -84,3 +84,19 @@ def test_autograd_function_and_refinement(cuda):
     err0 = (p0[:, 0].cpu().numpy() - truth[:, 0]) / scales[:, 0]
     err1 = (out[:, 0].detach().cpu().numpy() - truth[:, 0]) / scales[:, 0]
     assert np.median(np.abs(err1)) < np.median(np.abs(err0))
+
+
+def test_pack_curves_weights_equal_the_host_formula():
+    """refine.pack_curves forms w = 1 / (dy * dy) where the tensors live (here
+    on the CPU): bitwise the host NumPy values, with t, y and the offsets
+    concatenated in curve order."""
+    from gtls_b200 import refine
+    rng = np.random.default_rng(2)
+    curves = [(np.sort(rng.uniform(0, 10, n)), rng.normal(1, 1e-3, n), rng.uniform(1e-4, 3e-3, n))
+              for n in (5, 17, 1000)]
+    t, y, w, off = refine.pack_curves(curves, "cpu")
+    dy = np.concatenate([c[2] for c in curves])
+    np.testing.assert_array_equal(w.numpy(), 1.0 / (dy * dy))
+    np.testing.assert_array_equal(t.numpy(), np.concatenate([c[0] for c in curves]))
+    np.testing.assert_array_equal(y.numpy(), np.concatenate([c[1] for c in curves]))
+    np.testing.assert_array_equal(off.numpy(), [0, 5, 22, 1022])
