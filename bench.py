@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--chunk-mb", type=int, default=0,
                     help="per-chunk scratch budget of the searches in MiB (default: the library's 8 GiB)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the leg that times the reference's own kernels on the same GPU")
     ap.add_argument("--max-periods", type=int, default=0,
                     help="profiling only: keep this many periods spread over the grid (a smaller case of the "
                          "same kernels); the line then describes that case")
@@ -81,18 +83,8 @@ def traffic_per_period(precision, workload):
 
 def durations_step_for(periods, n, want):
     """duration_grid_step giving exactly ``want`` durations."""
-    from gtls_b200.grid import duration_grid
-    lo, hi = 1.0001, 3.0
-    for _ in range(200):
-        mid = 0.5 * (lo + hi)
-        c = len(duration_grid(periods, shortest=1 / n, log_step=mid))
-        if c > want:
-            lo = mid
-        elif c < want:
-            hi = mid
-        else:
-            return mid
-    raise RuntimeError("no duration step gives %d durations" % want)
+    from gtls_b200.grid import duration_grid_step_for
+    return duration_grid_step_for(periods, 1 / n, want)
 
 
 def workload(name, rank=0):
@@ -219,6 +211,81 @@ def cpu_reference(t, y, dy, periods, kw, step, batch_hint, budget_s=15.0, seed=0
                        "kernels compiled for the CPU (oracle/_ref, OpenMP, %d threads), extrapolated to %d + 206 "
                        "periods" % (main_n, all_n, os.cpu_count(), len(periods)),
                 seconds_per_curve=total)
+
+
+def pipe_object(timings, chi2_ms, precision):
+    """FMA-pipe figures of the main-pass chi2 kernel: 2 FLOP per multiply-add,
+    against the nominal FP64 (64 FMA/clk/SM) or FP32 (128) peak at 1.965 GHz.
+    ``dense``: every evaluated (start, template sample), whether or not the
+    start's window passes the depth test; ``active``: the starts that pass it,
+    the only sums that enter the result (the reference's kernel runs its
+    in-transit loop for these alone, GPUFun.py:409-424); ``issued``: what the
+    kernel executed (register groups of consecutive starts covering the
+    passing ones, padded template blocks)."""
+    peak = 148 * (64 if precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
+    sec = chi2_ms * 1e-3
+    out = {"unit": "TFLOP/s", "fp_pipe": "fp64" if precision == "fp64" else "fp32", "nominal_peak": peak,
+           "flops": "2 per (start, template sample) for B and for C"}
+    for key, name in (("chi2_fma", "dense"), ("chi2_active_fma", "active"), ("chi2_issued_fma", "issued")):
+        f = 2.0 * statistics.mean(tm[key] for tm in timings)
+        out[name + "_flops_per_step"] = f
+        out[name + "_tflops"] = f / sec / 1e12
+        out[name + "_frac"] = f / sec / 1e12 / peak
+    out["achieved"] = out["issued_tflops"]
+    out["frac"] = out["issued_frac"]
+    return out
+
+
+def ref_gpu_leg(cur, t, y, dy, lc, ov, periods, batch, ours_main_s, device, n_sample=6):
+    """The reference's own kernels on the same GPU: GPUFun.cu compiled for
+    sm_100a (oracle/_ref/libgpufun_ref_sm100.so), launched in the order of its
+    type-consistent caller (_worker.py, FP32 flux/weights/sums, torch playing
+    cupy's argsort/cumsum/argmin).  A stratified sample of its batches of
+    ``batch`` periods is timed (wall clock per batch: the reference reads the
+    batch's duration union back to the host every batch) and the main pass is
+    extrapolated to all batches.  The sampled periods are also searched here
+    in FP64 over the same batches, to compare chi2 minima and locations."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu as RG
+    import torch
+    from gtls_b200 import _lib
+    if not RG.available():
+        return None
+    rg = RG.RefGpuMainPass(t, y, dy, lc, ov, 1e-5, device)
+    rg.prepare(periods, batch)
+    nb = rg.n_batches
+    pick = np.unique(np.linspace(0, nb - 1, min(n_sample, nb)).astype(int))
+    rg.run_batch(int(pick[-1]))   # warm-up: module load, allocations
+    torch.cuda.synchronize()
+    times, same, total, rel = [], 0, 0, []
+    for b in pick:
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        out = rg.run_batch(int(b))
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - a)
+        if out is None:
+            continue
+        v, loc = out
+        s0, s1 = int(b) * batch, min((int(b) + 1) * batch, len(periods))
+        c, l = cur.search(periods[s0:s1], 1e-5, 8, batch, _lib.GTLS_PASS_MAIN, "fp64", want_loc=True)
+        v = v.double().cpu().numpy()
+        c = c.cpu().numpy()
+        same += int(np.sum(loc.cpu().numpy() == l.cpu().numpy()))
+        total += s1 - s0
+        rel.append(float(np.max(np.abs(v / c - 1))))
+    main_s = float(np.mean(times)) * nb
+    del rg
+    torch.cuda.empty_cache()
+    return {"what": "the reference's kernels (GPUFun.cu, SKIP_POINT 8) compiled for sm_100a and launched as its "
+                    "type-consistent caller _worker.py does (R32: FP64 times and phases, FP32 flux, weights and "
+                    "sums); torch plays cupy's argsort, cumsum, argmin and logical_or on the same stream; main "
+                    "pass only",
+            "batches": int(nb), "batch_periods": int(batch), "sampled_batches": [int(b) for b in pick],
+            "sampled_batch_s": times, "main_pass_s_extrapolated": main_s, "ours_main_pass_s": ours_main_s,
+            "main_pass_speedup": main_s / ours_main_s,
+            "r32_vs_ours_fp64": {"periods": total, "same_argmin_location": same / max(total, 1),
+                                 "max_rel_chi2_difference": max(rel) if rel else None}}
 
 
 def bench_refine(args):
@@ -494,9 +561,6 @@ def bench_batch(args):
     except (OSError, KeyError, ValueError):
         hbm_peak, peak_src = 6650.0, "fallback"
     achieved = 24.0 * work / (chi2_ms * 1e-3) / 1e9
-    flops = 2.0 * statistics.mean(t["chi2_fma"] for t in timings)
-    pipe_tflops = flops / (chi2_ms * 1e-3) / 1e12
-    pipe_peak = 148 * (64 if args.precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
     chunks = timings[0]["chunks"]
     line = {
         "metric": CFG4_METRIC, "value": len(idx) * 1000.0 / ms, "unit": "light curves/s", "n_gpus": 1,
@@ -515,8 +579,7 @@ def bench_batch(args):
                      "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
                      "launches_per_step": chunks, "avg_launch_ms": chi2_ms / max(chunks, 1),
                      "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64"},
-        "pipe": {"unit": "TFLOP/s", "fp_pipe": "fp64" if args.precision == "fp64" else "fp32",
-                 "achieved": pipe_tflops, "nominal_peak": pipe_peak, "frac": pipe_tflops / pipe_peak},
+        "pipe": pipe_object(timings, chi2_ms, args.precision),
         "stages_ms": {k: statistics.mean(t[k] for t in timings) for k in
                       ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
     }
@@ -803,10 +866,6 @@ def main():
         hbm_peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         hbm_peak, peak_src = 6650.0, "fallback"
-    flops = 2.0 * statistics.mean(tm["chi2_fma"] for tm in timings)
-    pipe_tflops = flops / (chi2_ms * 1e-3) / 1e12
-    pipe_peak = 148 * (64 if args.precision == "fp64" else 128) * 2 * 1.965e9 / 1e12
-
     tpp = traffic_per_period(args.precision, args.workload)
     chunk_periods = len(periods) / max(chunks, 1)
     line = {
@@ -828,9 +887,7 @@ def main():
                      "avg_launch_ms": chi2_ms / max(chunks, 1),
                      "algorithmic_bytes": "24*N per (curve, period): t, y, w in FP64",
                      "algorithmic_bytes_per_launch": bytes_per_period * chunk_periods},
-        "pipe": {"unit": "TFLOP/s", "fp_pipe": "fp64" if args.precision == "fp64" else "fp32",
-                 "achieved": pipe_tflops, "nominal_peak": pipe_peak, "frac": pipe_tflops / pipe_peak,
-                 "flops": "2 per (start, template sample) for B and for C"},
+        "pipe": pipe_object(timings, chi2_ms, args.precision),
         "stages_ms": {k: statistics.mean(tm[k] for tm in timings) for k in
                       ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")},
         "phases_ms": {"what": "one extra untimed search, wall clock per phase with a device synchronisation at "
@@ -844,6 +901,12 @@ def main():
     }
     if rank == 0:
         line["clocks"] = clk.summary()
+        if not args.no_ref_gpu and world == 1:
+            main_s = sum(statistics.mean(tm[k] for tm in timings)
+                         for k in ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")) / 1000.0
+            rgl = ref_gpu_leg(cur, t, y, dy, lc, ov, periods, batch, main_s, device)
+            if rgl is not None:
+                line["ref_gpu"] = rgl
         if not args.no_cpu_baseline:
             cb = cpu_reference(t, y, dy, periods, kw, step, batch)
             if cb is not None:

@@ -14,7 +14,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgtls_b200.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 GTLS_FP64, GTLS_FP32 = 0, 1
 GTLS_PASS_MAIN, GTLS_PASS_ALL = 0, 1
 GTLS_SEARCH_ALL_DURATIONS = 1
@@ -54,6 +54,8 @@ class Timing(ctypes.Structure):
         ("finish_ms", ctypes.c_double),
         ("chi2_starts", ctypes.c_int64),
         ("chi2_fma", ctypes.c_int64),
+        ("chi2_active_fma", ctypes.c_int64),
+        ("chi2_issued_fma", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -134,6 +136,7 @@ EXPORTS = {
     "gtls_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
     "gtls_abi_version": ([], ctypes.c_int),
     "gtls_launch_count": ([ctypes.c_void_p], ctypes.c_int64),
+    "gtls_decode_status": ([ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
     "gtls_set_chunk_budget": ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_int),
     "gtls_set_tuning": ([ctypes.c_void_p, ctypes.POINTER(Tuning)], ctypes.c_int),
     "gtls_get_tuning": ([ctypes.c_void_p, ctypes.POINTER(Tuning)], ctypes.c_int),
@@ -199,6 +202,16 @@ def _check(rc, ctx, what):
     if rc != 0:
         msg = load().gtls_last_error(ctx).decode(errors="replace")
         raise GtlsError("%s failed (%d): %s" % (what, rc, msg))
+
+
+def device_status_error(word):
+    """GtlsError for a non-zero device status word of a search (its meaning
+    from gtls_decode_status), None for 0."""
+    buf = ctypes.create_string_buffer(256)
+    rc = load().gtls_decode_status(int(word), buf, len(buf))
+    if rc == 0:
+        return None
+    return GtlsError("device status %d (%d): %s" % (int(word), rc, buf.value.decode(errors="replace")))
 
 
 def _torch():

@@ -259,6 +259,19 @@ int gtls_set_chunk_budget(gtls_ctx* ctx, uint64_t bytes) {
   return GTLS_OK;
 }
 
+int gtls_decode_status(int32_t word, char* msg, size_t cap) {
+  std::string m;
+  if (word == 0) m = "ok";
+  if (word & 1) m += "chi2 kernel: shared-memory tile copy did not complete within its bounded wait";
+  if (word & ~1) m += (m.empty() ? "" : "; ") + std::string("unknown device status bits ") + std::to_string(word & ~1);
+  if (msg && cap > 0) {
+    const size_t k = std::min(cap - 1, m.size());
+    std::memcpy(msg, m.data(), k);
+    msg[k] = 0;
+  }
+  return word == 0 ? GTLS_OK : GTLS_E_DEVICE;
+}
+
 const char* gtls_last_error(const gtls_ctx* ctx) {
   return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }

@@ -56,6 +56,11 @@ constexpr int kSmallBucket = 8;     // entries of buckets up to this size are ra
 constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (warp-ranked)
 constexpr int kChiThreads = 512;
 constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset rho
+// Split-path task: a window of kWin consecutive starts of one duration.  Its
+// starts are first put through the depth test; the starts that pass are then
+// covered by groups of kR consecutive starts (each beginning at the first
+// uncovered start that passes), and only those groups are correlated.
+constexpr int kWin = 4 * kR;
 // Zeroed records after each shared-memory tile: a skip-1 group whose kR
 // starts all lie in the tile reads at most kR - 2 records past it (only ever
 // against zero template entries), so those groups need no clamping.
@@ -468,6 +473,7 @@ struct Chi2Args {
   int* status;              // device status word (bit 0: tile copy did not complete)
   double* part_v;           // [chunk tiles]
   long long* part_loc;      // [chunk tiles]
+  unsigned long long* work; // NULL, or [2]: multiply-adds of the starts passing the depth test, and issued
 };
 
 // Mean depth of the window [k, k+w): -(sum v)/w  (calcAverageFromCumsum, GPUFun.py:366-375),
@@ -619,6 +625,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   __shared__ Best red[kChiThreads / 32];
   __shared__ __align__(8) uint64_t tile_bar;
   __shared__ int tile_ok;
+  __shared__ unsigned long long work_sm[2];
 
   const int cta = blockIdx.x;
   const int ri = upper_find(0, a.nruns, cta, [&](int i) { return (long long)runs[i].tile0; });
@@ -675,7 +682,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
         const int sk = skips[d];
         const int jlo = (k0 + sk - 1) / sk, jhi = (k1 + sk - 1) / sk;
         const int nj = max(0, jhi - jlo);
-        nt = (sk >= kSplitMinSkip) ? (nj + kR - 1) / kR : (nj + 32 * kR - 1) / (32 * kR);
+        nt = (sk >= kSplitMinSkip) ? (nj + kWin - 1) / kWin : (nj + 32 * kR - 1) / (32 * kR);
       }
       int inc = nt;
 #pragma unroll
@@ -689,11 +696,19 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     if (lane == 0) {
       task_pre[ucnt] = carry;
       task_next = 0;
+      work_sm[0] = work_sm[1] = 0;
       if constexpr (kGlobal) {
         tile_ok = 1;
       } else {
         tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
-        if (!tile_ok) atomicOr(a.status, 1);
+        if (!tile_ok) {
+          // The copy into this CTA's shared memory may still be in flight:
+          // record the failure, then wait for it again (bounded, 16x longer)
+          // before the CTA goes on to evaluate nothing and exit, so that the
+          // copy does not land in shared memory that a later CTA owns.
+          atomicOr(a.status, 1);
+          mbar_wait_bounded(&tile_bar, 0, 1LL << 26);
+        }
       }
     }
   }
@@ -721,6 +736,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       }
   }
   const int ntask = tile_ok ? task_pre[ucnt] : 0;
+  const bool count_work = a.work != nullptr;
   while (true) {
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&task_next, 1);
@@ -747,45 +763,72 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     const Real os = dtab_os[d];
     const Real inv_w = (Real)1 / (Real)w;
     const long long locb = (long long)upos * n;
+    const int Qr = (Q + kR - 1) / kR * kR;
     R2 acc[kR];
-#pragma unroll
-    for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
     if (s >= kSplitMinSkip) {
-      // lanes split the offset rho inside a skip block; one task = kR starts
-      const int jb = jlo + sub * kR;
-      // every load of the task inside the tile: no clamping needed
-      const int Qr = (Q + kR - 1) / kR * kR;
-      if ((jb + Qr + kR - 1) * s - k0 <= L) {
-        if (!kTwoLevel && Qr == kR) {
-          correlate_rounds<Real>(recs, jb * s - k0, s, trow, lane, acc);
+      // lanes split the offset rho inside a skip block.  (1) the depth test
+      // of the window's starts (one start per lane); a start that fails it
+      // takes the value n here and needs no sums (GPUFun.py:407,437)
+      const int jw = jlo + sub * kWin;
+      const int jend = min(jhi, jw + kWin);
+      unsigned long long act = 0;
+#pragma unroll
+      for (int i0 = 0; i0 < kWin; i0 += 32) {
+        const int j = jw + i0 + lane;
+        bool on = false;
+        if (i0 + lane < kWin && j < jend) {
+          const int k = j * s;
+          on = (double)window_mean(pre, k, w, inv_w) > a.depth_min;
+          if (!on) best_update(best, sentinel, locb + k);
+        }
+        act |= (unsigned long long)__ballot_sync(0xffffffffu, on) << i0;
+      }
+      if (count_work && lane == 0) atomicAdd(&work_sm[0], (unsigned long long)__popcll(act) * 2ULL * (unsigned)w);
+      // (2) groups of kR consecutive starts, each from the first start of the
+      //     window that passes and is not yet covered (moved back so that it
+      //     ends inside the window: the starts it then re-covers are either
+      //     covered already or fail the test)
+      while (act) {
+        const int off = min(__ffsll((long long)act) - 1, kWin - kR);
+        act &= ~(((1ULL << kR) - 1ULL) << off);
+        const int jb = jw + off;
+#pragma unroll
+        for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
+        // every load of the group inside the tile: no clamping needed
+        if ((jb + Qr + kR - 1) * s - k0 <= L) {
+          if (!kTwoLevel && Qr == kR) {
+            correlate_rounds<Real>(recs, jb * s - k0, s, trow, lane, acc);
+          } else {
+            for (int rho = lane; rho < s; rho += 32)
+              correlate_pre<Real, kTwoLevel, false>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+          }
         } else {
           for (int rho = lane; rho < s; rho += 32)
-            correlate_pre<Real, kTwoLevel, false>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+            correlate_pre<Real, kTwoLevel, true>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
-      } else {
-        for (int rho = lane; rho < s; rho += 32)
-          correlate_pre<Real, kTwoLevel, true>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
-      }
-      const Real mine = warp_reduce_scatter18<Real>(acc);
-      // lane kLaneOf[r] holds B_r, lane kLaneOf[kR + r] holds C_r
-      int r = -1;
+        if (count_work && lane == 0) atomicAdd(&work_sm[1], (unsigned long long)kR * 2ULL * (unsigned)(Qr * s));
+        const Real mine = warp_reduce_scatter18<Real>(acc);
+        // lane kLaneOf[r] holds B_r, lane kLaneOf[kR + r] holds C_r
+        int r = -1;
 #pragma unroll
-      for (int i = 0; i < kR; ++i)
-        if (lane == kLaneOf[i]) r = i;
-      const int srcl = r >= 0 ? kLaneOf[kR + r] : lane;
-      const Real C = __shfl_sync(0xffffffffu, mine, srcl);
-      if (r >= 0) {
-        const int j = jb + r;
-        if (j < jhi) {
-          const int k = j * s;
-          eval_start<Real>(best, pre, k, w, inv_w, os, mine, C, a.depth_min, ebase, sentinel, locb + k);
+        for (int i = 0; i < kR; ++i)
+          if (lane == kLaneOf[i]) r = i;
+        const int srcl = r >= 0 ? kLaneOf[kR + r] : lane;
+        const Real C = __shfl_sync(0xffffffffu, mine, srcl);
+        if (r >= 0) {
+          const int j = jb + r;
+          if (j < jend) {
+            const int k = j * s;
+            eval_start<Real>(best, pre, k, w, inv_w, os, mine, C, a.depth_min, ebase, sentinel, locb + k);
+          }
         }
       }
     } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
       // each lane takes kR consecutive start blocks and every rho
       const int jb = jlo + (sub * 32 + lane) * kR;
       if (jb < jhi) {
-        const int Qr = (Q + kR - 1) / kR * kR;
         if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
           correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
         } else {
@@ -812,6 +855,21 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
           }
         }
       }
+      if (count_work) {
+        // work counters: the lanes' starts, and those passing the depth test
+        unsigned nst = 0, nact = 0;
+        if (jb < jhi)
+          for (int r = 0; r < kR && jb + r < jhi; ++r) {
+            ++nst;
+            nact += (double)window_mean(pre, (jb + r) * s, w, inv_w) > a.depth_min;
+          }
+        nst = __reduce_add_sync(0xffffffffu, nst);
+        nact = __reduce_add_sync(0xffffffffu, nact);
+        if (lane == 0) {
+          atomicAdd(&work_sm[0], (unsigned long long)nact * 2ULL * (unsigned)w);
+          atomicAdd(&work_sm[1], (unsigned long long)((nst + kR - 1) / kR * kR) * 2ULL * (unsigned)(Qr * s));
+        }
+      }
     }
   }
   // CTA minimum (value, then location)
@@ -828,6 +886,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     for (int i = 1; i < kChiThreads / 32; ++i) best_update(b, red[i].v, red[i].loc);
     a.part_v[cta] = b.v;
     a.part_loc[cta] = b.loc;
+    if (a.work) {
+      atomicAdd(a.work, work_sm[0]);
+      atomicAdd(a.work + 1, work_sm[1]);
+    }
   }
 }
 
@@ -1189,6 +1251,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   carve_size<Pv>(total, max_pv);
   carve_size<double>(total, max_part);
   carve_size<long long>(total, max_part);
+  carve_size<unsigned long long>(total, 2);
   total += 32 * 256;
   void* mem = arena(ctx, total);
   if (!mem) return fail(ctx, GTLS_E_NOMEM, "scratch allocation failed");
@@ -1223,6 +1286,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   Pv* pv = cv.take<Pv>(max_pv);
   double* part_v = cv.take<double>(max_part);
   long long* part_loc = cv.take<long long>(max_part);
+  unsigned long long* work = cv.take<unsigned long long>(2);
   {
     std::vector<long long> offs(3 * (size_t)(n_curves + 1));
     std::copy(p_off.begin(), p_off.end(), offs.begin());
@@ -1249,6 +1313,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     GTLS_TRY_CUDA(ctx, cudaEventRecord(ev[0], st));
   }
   GTLS_TRY_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(int), st));
+  if (tm) GTLS_TRY_CUDA(ctx, cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), st));
   curve_setup_kernel<Real><<<n_curves, 1024, 0, st>>>(d_cd);
   if (p_off[n_curves] > 0)
     duration_range_batch_kernel<Real><<<(unsigned)((p_off[n_curves] + 255) / 256), 256, 0, st>>>(d_cd, d_poff,
@@ -1282,6 +1347,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   ca.status = ctx->status;
   ca.part_v = part_v;
   ca.part_loc = part_loc;
+  ca.work = tm ? work : nullptr;
   for (int k = 0; k < nchunks; ++k) {
     const int r0 = chunk_r0[k], nr = chunk_r0[k + 1] - r0;
     const int items = chunk_items[k], tiles = chunk_tiles[k];
@@ -1343,12 +1409,19 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     }
     tm->chi2_starts = starts;
     tm->chi2_fma = fma;
+    unsigned long long hwk[2] = {0, 0};
+    GTLS_TRY_CUDA(ctx, cudaMemcpy(hwk, work, sizeof(hwk), cudaMemcpyDeviceToHost));
+    tm->chi2_active_fma = (long long)hwk[0];
+    tm->chi2_issued_fma = (long long)hwk[1];
   }
   // device status word: a tile copy that did not complete within its bound
   int hst = 0;
   GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(&hst, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   GTLS_TRY_CUDA(ctx, cudaStreamSynchronize(st));
-  if (hst != 0) return fail(ctx, GTLS_E_DEVICE, "chi2 kernel: shared-memory tile copy timed out");
+  if (hst != 0) {
+    char msg[200];
+    return fail(ctx, gtls_decode_status(hst, msg, sizeof(msg)), msg);
+  }
   return GTLS_OK;
 }
 

@@ -4,11 +4,12 @@ Follows the reference's ``src/gputls/grid.py``: ``T14`` (:7-29),
 ``duration_grid`` (:32-53) and ``period_grid`` (:56-157, Ofir 2014 optimal
 frequency sampling).  The scalar set-up (stellar-parameter clamps, the Ofir
 coefficients A and C, the number of grid points) runs on the host exactly as
-in the reference; the per-point evaluation ``P(X) = 1 / (A/3*X + C)^3 / 86400``
-and the selection of ``period_min < P <= period_max`` run on the GPU
-(``gtls_period_grid`` in the C-ABI).  The device evaluates the cube correctly
-rounded, so each period is within 1 ulp of NumPy's ``**3`` (whose SIMD pow
-rounding depends on the host CPU).
+in the reference.  The per-point evaluation ``P(X) = 1 / (A/3*X + C)^3 / 86400``
+and the selection of ``period_min < P <= period_max`` run either on the host
+with the reference's own NumPy expression (the default: bit-identical to the
+reference's grid on the same host, whose NumPy ``**3`` rounding depends on
+the CPU's SIMD pow) or on the GPU (``gtls_period_grid`` in the C-ABI, the cube
+correctly rounded, so each period within 2 ulp of NumPy's).
 """
 import warnings
 
@@ -47,6 +48,23 @@ def duration_grid(periods, shortest, log_step=constants.DURATION_GRID_STEP):
     return durations
 
 
+def duration_grid_step_for(periods, shortest, count):
+    """The ``log_step`` for which ``duration_grid(periods, shortest, log_step)``
+    has exactly ``count`` durations (bisection; the count falls as the step
+    grows).  Workloads that ask for a number of durations use it."""
+    lo, hi = 1.0001, 3.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        c = len(duration_grid(periods, shortest=shortest, log_step=mid))
+        if c > count:
+            lo = mid
+        elif c < count:
+            hi = mid
+        else:
+            return mid
+    raise ValueError("no duration grid step gives %d durations" % count)
+
+
 def ofir_coefficients(R_star, M_star, time_span, oversampling_factor=constants.OVERSAMPLING_FACTOR,
                       n_transits_min=constants.N_TRANSITS_MIN):
     """Clamp the stellar parameters and return (A/3, C, n_points) of the Ofir grid.
@@ -79,21 +97,38 @@ def ofir_coefficients(R_star, M_star, time_span, oversampling_factor=constants.O
     return np.float64(A / 3), np.float64(C), int(n_points), time_span
 
 
+def _host_points(a3, c, n_points, period_min, period_max):
+    """grid.py:127-133: f_x = (A/3 * X + C)^3, P = 1/f_x/86400, kept where
+    period_min < P <= period_max; the same NumPy operations in the same order
+    (so the same bits on the same host).  Ascending."""
+    X = np.arange(n_points, dtype=np.float64) + 1
+    f_x = (a3 * X + c) ** 3
+    periods = 1 / f_x / constants.SECONDS_PER_DAY
+    sel = np.where(np.logical_and(periods > period_min, periods <= period_max))
+    return np.ascontiguousarray(periods[sel][::-1])
+
+
 def period_grid(R_star, M_star, time_span, period_min=0, period_max=float("inf"),
                 oversampling_factor=constants.OVERSAMPLING_FACTOR,
-                n_transits_min=constants.N_TRANSITS_MIN, device=0, ascending=False):
-    """Ofir-optimal trial periods in days, evaluated on the GPU.
+                n_transits_min=constants.N_TRANSITS_MIN, device=0, ascending=False, evaluate="host"):
+    """Ofir-optimal trial periods in days.
 
-    Returns the periods in the reference's order (descending, as
-    grid.py:132-157 returns them) unless ``ascending`` is set.  With fewer
-    than 100 periods the grid is rebuilt for R_star = M_star = 1 and a time
-    span of at least 5 days, with the default bounds, as the reference does.
+    ``evaluate``: "host" (default) evaluates the points with the reference's
+    NumPy expression, "device" on the GPU (``gtls_period_grid``).  Returns
+    the periods in the reference's order (descending, as grid.py:132-157
+    returns them) unless ``ascending`` is set.  With fewer than 100 periods
+    the grid is rebuilt for R_star = M_star = 1 and a time span of at least 5
+    days, with the default bounds, as the reference does.
     """
-    from . import _lib
-
+    if evaluate not in ("host", "device"):
+        raise ValueError("evaluate must be 'host' or 'device'")
     a3, c, n_points, span_s = ofir_coefficients(R_star, M_star, time_span, oversampling_factor,
                                                 n_transits_min)
-    periods = _lib.period_grid(a3, c, n_points, float(period_min), float(period_max), device=device)
+    if evaluate == "host":
+        periods = _host_points(a3, c, n_points, period_min, period_max)
+    else:
+        from . import _lib
+        periods = _lib.period_grid(a3, c, n_points, float(period_min), float(period_max), device=device)
     if periods.size > 10 ** 6:
         warnings.warn("period_grid generates a very large grid (" + str(periods.size)
                       + "). Recommend to check physical plausibility for stellar mass, radius, "
@@ -104,5 +139,5 @@ def period_grid(R_star, M_star, time_span, period_min=0, period_max=float("inf")
         warnings.warn("period_grid defaults to R_star=1 and M_star=1 as given density yielded grid "
                       "with too few values")
         return period_grid(R_star=1, M_star=1, time_span=span_s / constants.SECONDS_PER_DAY,
-                           device=device, ascending=ascending)
+                           device=device, ascending=ascending, evaluate=evaluate)
     return periods if ascending else periods[::-1].copy()

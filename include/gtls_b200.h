@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define GTLS_ABI_VERSION 1
+#define GTLS_ABI_VERSION 2
 
 enum gtls_status {
   GTLS_OK = 0,
@@ -60,6 +60,16 @@ const char* gtls_last_error(const gtls_ctx* ctx);
 
 /* ABI version compiled into the library (GTLS_ABI_VERSION). */
 int gtls_abi_version(void);
+
+/* Meaning of a search's device status word (no counterpart in the
+ * reference, whose kernels have no error path).  The search kernels set bits
+ * of a per-context word instead of hanging: bit 0 = a chi2 CTA's
+ * shared-memory tile copy did not complete within its bounded wait (the CTA
+ * then waited, bounded again, for the copy in flight, evaluated nothing and
+ * left its period's minimum at +inf).  Returns GTLS_OK for 0 and
+ * GTLS_E_DEVICE otherwise, and writes a NUL-terminated message of at most
+ * `cap` bytes to `msg` (host; msg may be NULL). */
+int gtls_decode_status(int32_t word, char* msg, size_t cap);
 
 /* Number of kernels this context has launched since it was created
  * (no counterpart in the reference; used to account for device work). */
@@ -136,7 +146,16 @@ typedef struct gtls_timing {
   double chi2_ms;             /* chi2 kernel, all chunks                        */
   double finish_ms;           /* per-period minimum, all chunks                 */
   int64_t chi2_starts;        /* (duration, start) evaluations done by the chi2 kernel */
-  int64_t chi2_fma;           /* multiply-adds of B and C issued by the chi2 kernel */
+  int64_t chi2_fma;           /* multiply-adds of B and C over every evaluated start
+                                 (2 * width per start, whether or not its window
+                                 passes the depth test)                          */
+  int64_t chi2_active_fma;    /* the same over the starts whose window mean passes
+                                 the depth test: the only starts whose sums enter
+                                 the result (the reference's in-transit loop runs
+                                 for these alone, GPUFun.py:409-424)            */
+  int64_t chi2_issued_fma;    /* multiply-adds the kernel performed (register
+                                 groups of consecutive starts, padded template
+                                 blocks included)                                */
 } gtls_timing;
 
 /*

@@ -62,3 +62,19 @@ def test_ctypes_descriptors_match_the_c_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_device_status_word_becomes_an_error():
+    """A search's non-zero device status word (a chi2 tile copy that did not
+    complete within its bounded wait) is reported as GTLS_E_DEVICE with its
+    meaning, and the Python layer turns it into GtlsError; 0 is no error."""
+    from gtls_b200 import _lib
+    lib = _lib.load()
+    buf = ctypes.create_string_buffer(128)
+    assert lib.gtls_decode_status(0, buf, len(buf)) == 0
+    assert lib.gtls_decode_status(1, buf, len(buf)) == 5   # GTLS_E_DEVICE
+    assert b"tile copy" in buf.value
+    assert lib.gtls_decode_status(5, buf, 16) == 5 and len(buf.value) == 15   # truncated, NUL-terminated
+    assert _lib.device_status_error(0) is None
+    err = _lib.device_status_error(1)
+    assert isinstance(err, _lib.GtlsError) and "tile copy" in str(err)

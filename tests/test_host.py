@@ -54,6 +54,18 @@ def test_ofir_coefficients_reproduce_reference_grid_within_one_ulp():
             np.testing.assert_array_almost_equal_nulp(p, ref, nulp=1)
 
 
+def test_default_period_grid_is_bitwise_the_reference_grid():
+    """The default (host) evaluation of power()'s grid: the reference's
+    grid.period_grid outputs bit for bit, fallback grids included."""
+    g = golden("grid")
+    for i in range(6):
+        rs, ms, span, pmin, pmax, osf, ntr = g["case%d_args" % i]
+        ours = G.period_grid(rs, ms, span, pmin, pmax, int(osf), int(ntr))
+        np.testing.assert_array_equal(ours, g["case%d_periods" % i])
+        asc = G.period_grid(rs, ms, span, pmin, pmax, int(osf), int(ntr), ascending=True)
+        np.testing.assert_array_equal(asc, g["case%d_periods" % i][::-1])
+
+
 def test_template_cache_matches_reference_get_cache():
     c = golden("cache")
     for i in range(2):
