@@ -144,7 +144,9 @@ class gtls_batch(object):
     True adds transit times and the SNRs) and ``keep_spectra`` (default
     True: each result carries its periods, power and chi2) and ``autotune``
     (default True: launch shapes timed and chosen on the data, see
-    ``gtls_b200.tune``; results do not depend on them).  With
+    ``gtls_b200.tune``; results do not depend on them); ``refine=True``
+    refines every curve's best peak in one batched adjoint run (see
+    ``refine_results``).  With
     ``distributed=True`` under an initialised torch.distributed process group
     (one process per GPU) every rank searches a work-balanced share of the
     curves and all ranks return every curve's result."""
@@ -179,8 +181,13 @@ class gtls_batch(object):
             ph = core.Phases(phases)
             prepared = [prepare_curve(*self.curves[i], sub, device=device) for i in indices]
             ph.mark("prepare_curves")
-            return search_prepared(prepared, sub, device=device, full_stats=full_stats,
-                                   keep_spectra=keep_spectra, timing=timing, autotune=autotune, phases=phases)
+            out = search_prepared(prepared, sub, device=device, full_stats=full_stats,
+                                  keep_spectra=keep_spectra, timing=timing, autotune=autotune, phases=phases)
+            if opts.refine and out:
+                ph = core.Phases(phases)
+                refine_results(out, prepared, opts.u, device)
+                ph.mark("refine")
+            return out
 
         if opts.distributed:
             # each rank searches a share of the curves balanced by estimated
@@ -189,6 +196,28 @@ class gtls_batch(object):
             costs = [len(c[0]) * float(np.ptp(np.asarray(c[0], dtype=np.float64))) for c in self.curves]
             return shard.sharded_curves(costs, search_subset)
         return search_subset(list(range(len(self.curves))))
+
+
+def refine_results(out, prepared, u, device):
+    """power(refine=True): every curve's best peak refined in one batched run
+    of the adjoint of the limb-darkened model chi2 (``refine.refine_peaks``);
+    a result takes the refined period, T0, duration and depth only where the
+    model chi2 decreased, and ``r.refinement`` keeps both."""
+    from . import refine as R
+    starts, scales = [], []
+    for r, p in zip(out, prepared):
+        a, b = R.grid_start(r.period, r.T0, r.duration, r.depth, u, p["periods"], p["t"])
+        starts.append(a)
+        scales.append(b)
+    params, chi, chi0, ok = R.refine_peaks([(p["t"], p["y"], p["dy"]) for p in prepared], np.array(starts),
+                                           np.array(scales), device=device)
+    for c, r in enumerate(out):
+        r.refinement = dict(grid=dict(period=r.period, T0=r.T0, duration=r.duration, depth=r.depth),
+                            params=params[c], chi2=float(chi[c]), chi2_grid=float(chi0[c]), improved=bool(ok[c]))
+        if ok[c]:
+            r.period, r.T0, r.duration, r.depth = (float(v) for v in params[c][:4])
+            if hasattr(r, "transit_times"):
+                r.transit_times = R.refined_transit_times(r.transit_times, r.T0, r.period)
 
 
 def _recheck_fp64(cs, cand, cand_p, c_off, spectra, chi2_dev, p_off, S, depth_min, skip, torch):

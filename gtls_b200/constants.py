@@ -76,5 +76,5 @@ VALID_PARAMETERS = [
     "oversampling_factor", "T0_fit_margin", "use_threads", "show_progress_bar",
     "transit_template", "verbose", "bar_location",
     # additions of this implementation (no counterpart in the reference)
-    "precision", "batch_periods", "distributed", "useLocalPTXCUBIN",
+    "precision", "batch_periods", "distributed", "useLocalPTXCUBIN", "refine",
 ]

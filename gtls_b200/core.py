@@ -363,6 +363,17 @@ def finish_period(widths, durations, overshoot, maxd, span, period, loc, t, y, d
     width = int(w_sel[didx])
     raw_duration = float(durations[sel][didx])
     ovs = float(overshoot[sel][didx])
+    return finish_stats(t, y, period, loc, width, raw_duration, ovs, maxd, full_stats=full_stats)
+
+
+def finish_stats(t, y, period, loc, width, raw_duration, ovs, maxd, full_stats=True):
+    """Host statistics of the best period (core.py:1427-1499) given its chi2
+    minimum ``loc`` (= duration position * n + start), the width, duration
+    and overshoot of that duration: depth, T0, duration in days and, with
+    ``full_stats``, transit times, snr, snr_pink, snrFit and snrFitPink."""
+    t = np.asarray(t, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    n = len(t)
     phase = (t % period) / period                       # foldCPU core.py:16-20
     rank = np.argsort(phase)
     best_t = np.array(t[rank])

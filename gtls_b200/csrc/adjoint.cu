@@ -3,18 +3,27 @@
 // An addition with no counterpart in the reference: it refines a search
 // peak below the period/duration grid resolution.
 //
-// Model, for one light curve with parameters (P, T0, D, depth, u1, u2):
-//   n    = round((t - T0) / P)                 nearest transit epoch
-//   tau  = (t - T0) - n P                      time from mid-transit
-//   s    = 2 tau / D                           chord coordinate (|s| < 1 in transit)
-//   B(s) = sigmoid((1 - s^2) / kEdge)          smooth ingress/egress
-//   mu   = sqrt(softplus_k(1 - s^2))           cosine of the emission angle on the chord,
-//                                              softplus_k(x) = log(1 + exp(k x)) / k
-//   I(s) = 1 - u1 (1 - mu) - u2 (1 - mu)^2    quadratic limb darkening
-//   m(t) = 1 - depth * B(s) * I(s) / I(0)
-// chi2 = sum_i w_i (y_i - m(t_i))^2, w_i = 1/dy_i^2.  Every factor is smooth,
-// so the gradient is exact everywhere (n is locally constant: dtau/dP = -n).
-// The backward pass recomputes m and dm/dtheta per sample instead of storing them.
+// The model is the search's own template model (gtls_b200/ldmodel.py, which
+// stands in for the batman light curve of src/gputls/transit.py:8-42): a
+// central (impact parameter 0) transit on a circular orbit of an opaque disk
+// of radius p (stellar radii) across a star with quadratic limb darkening
+// I(r) = 1 - u1 (1 - mu) - u2 (1 - mu)^2, mu = sqrt(1 - r^2).  For one light
+// curve with parameters (P, T0, D, depth, u1, u2):
+//   K   = 1 - u1/3 - u2/6,  p = sqrt(depth K)     (depth = central depth)
+//   a   = (1 + p) / sin(pi D / P)                 (D = first-to-fourth contact)
+//   phi = 2 pi ((t - T0)/P - n),  n = round((t - T0)/P)
+//   z   = a |sin phi|            (no occultation when cos phi < 0)
+//   m   = 1 - lambda(z, p, u1, u2),
+// lambda = [int_0^{p-z} 2 pi r I dr + int_{|z-p|}^{min(1,z+p)} 2 r acos(c) I dr] / (pi K),
+// c = (r^2 + z^2 - p^2) / (2 r z), both integrals by 96-node Gauss-Legendre
+// quadrature after r = m + h sin(theta), exactly as ldmodel does.  Written as
+// lambda = (M0 - u1 M1 - u2 M2) / (pi K) with the moments Mk of (1 - mu)^k,
+// the u-derivatives are closed-form; the (z, p)-derivatives are those of the
+// discrete quadrature itself (dual numbers through the nodes, the limits and
+// c), so the gradient is exact for the model the forward pass evaluates.
+// chi2 = sum_i w_i (y_i - m(t_i))^2, w_i = 1/dy_i^2.  n is locally constant,
+// so dphi/dP = -2 pi (t - T0) / P^2.  The backward pass recomputes the model
+// per sample instead of storing it.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -24,69 +33,208 @@
 
 namespace gtls {
 
-constexpr double kEdge = 0.05;       // ingress/egress softness in chord units
-constexpr double kSoftK = 200.0;     // softplus sharpness of the limb
 constexpr int kAdjThreads = 256;
+constexpr int kGLN = 96;
+constexpr double kPi = 3.14159265358979323846;
+
+// Quadrature table: s[j] = sin(theta_j), jw[j] = cos(theta_j) * pi/2 * w_j
+// with theta_j = pi/2 x_j for the Gauss-Legendre nodes x_j and weights w_j.
+struct GLTable {
+  double s[kGLN];
+  double jw[kGLN];
+};
+
+// Gauss-Legendre nodes and weights on [-1, 1] by Newton's method on the
+// three-term recurrence of the Legendre polynomials (Golub-Welsch-free
+// classic; converges to a few ulp from the Tricomi starting values).
+static GLTable make_gl_table() {
+  GLTable g;
+  const int n = kGLN;
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double x = std::cos(kPi * (i + 0.75) / (n + 0.5));
+    double dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = x;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (x * p1 - p0) / (x * x - 1.0);
+      const double dx = p1 / dp;
+      x -= dx;
+      if (std::fabs(dx) < 1e-17) break;
+    }
+    const double w = 2.0 / ((1.0 - x * x) * dp * dp);
+    // ascending order: node j = n-1-i holds +x, node i holds -x
+    const int hi = n - 1 - i, lo = i;
+    const double th = 0.5 * kPi * x;
+    g.s[hi] = std::sin(th);
+    g.jw[hi] = std::cos(th) * (0.5 * kPi) * w;
+    g.s[lo] = -g.s[hi];
+    g.jw[lo] = g.jw[hi];
+  }
+  return g;
+}
+
+static const GLTable& gl_table() {
+  static const GLTable g = make_gl_table();
+  return g;
+}
+
+// value and derivatives with respect to (z, p)
+struct D2 {
+  double v, z, p;
+};
+__device__ __forceinline__ D2 d2(double v) { return {v, 0.0, 0.0}; }
+__device__ __forceinline__ D2 operator+(D2 a, D2 b) { return {a.v + b.v, a.z + b.z, a.p + b.p}; }
+__device__ __forceinline__ D2 operator-(D2 a, D2 b) { return {a.v - b.v, a.z - b.z, a.p - b.p}; }
+__device__ __forceinline__ D2 operator*(D2 a, D2 b) {
+  return {a.v * b.v, a.v * b.z + b.v * a.z, a.v * b.p + b.v * a.p};
+}
+__device__ __forceinline__ D2 operator*(D2 a, double s) { return {a.v * s, a.z * s, a.p * s}; }
+__device__ __forceinline__ D2 operator/(D2 a, D2 b) {
+  const double q = a.v / b.v;
+  return {q, (a.z - q * b.z) / b.v, (a.p - q * b.p) / b.v};
+}
+// value of double inputs: the same expressions without derivatives
+__device__ __forceinline__ double dval(double a) { return a; }
+__device__ __forceinline__ double dval(D2 a) { return a.v; }
+
+// mu = sqrt(max(1 - r^2, 0)) and its derivative (0 where clamped)
+__device__ __forceinline__ double mu_of(double r) {
+  const double x = 1.0 - r * r;
+  return x > 0.0 ? sqrt(x) : 0.0;
+}
+__device__ __forceinline__ D2 mu_of(D2 r) {
+  const double x = 1.0 - r.v * r.v;
+  if (!(x > 0.0)) return d2(0.0);
+  const double m = sqrt(x);
+  const double k = -r.v / m;
+  return {m, k * r.z, k * r.p};
+}
+// acos of c clamped to [-1, 1] (derivative 0 where clamped)
+__device__ __forceinline__ double acos_clamped(double c) {
+  return c >= 1.0 ? 0.0 : (c <= -1.0 ? kPi : acos(c));
+}
+__device__ __forceinline__ D2 acos_clamped(D2 c) {
+  if (c.v >= 1.0) return d2(0.0);
+  if (c.v <= -1.0) return d2(kPi);
+  const double s = 1.0 - c.v * c.v;
+  const double k = s > 0.0 ? -1.0 / sqrt(s) : 0.0;
+  return {acos(c.v), k * c.z, k * c.p};
+}
+
+// Constants of either scalar type.
+template <typename T> __device__ __forceinline__ T cst(double v);
+template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
+template <> __device__ __forceinline__ D2 cst<D2>(double v) { return d2(v); }
+
+// Moments M0..M2 of the occulted flux: lambda = (M0 - u1 M1 - u2 M2) / (pi K),
+// Mk = int (1 - mu)^k x (2 pi r over the covered disk, 2 r acos(c) over the
+// partly covered annuli) dr, both by the quadrature of ldmodel.occulted_fraction.
+template <typename T>
+__device__ __forceinline__ void occultation_moments(T Z, T Pp, const GLTable& g, T (&M)[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) M[k] = cst<T>(0.0);
+  const double z = dval(Z), p = dval(Pp);
+  const T one = cst<T>(1.0);
+  // region fully covered by the planet: r in [0, min(p - z, 1)]
+  if (p - z > 0.0) {
+    const T ih = p - z > 1.0 ? one : Pp - Z;
+    const T half = ih * 0.5;
+    for (int j = 0; j < kGLN; ++j) {
+      const T r = half + half * g.s[j];
+      const T wt = half * g.jw[j];
+      const T om = one - mu_of(r);
+      const T f = r * wt * (2.0 * kPi);
+      M[0] = M[0] + f;
+      M[1] = M[1] + f * om;
+      M[2] = M[2] + f * om * om;
+    }
+  }
+  // partially covered annuli: r in [|z - p|, min(1, z + p)]
+  const T lo = z >= p ? Z - Pp : Pp - Z;
+  const T hi = z + p > 1.0 ? one : Z + Pp;
+  if (dval(hi) > dval(lo)) {
+    const T mid = (lo + hi) * 0.5;
+    const T half = (hi - lo) * 0.5;
+    const T zs = z > 1e-300 ? Z : cst<T>(1e-300);
+    const T zp2 = zs * zs - Pp * Pp;
+    for (int j = 0; j < kGLN; ++j) {
+      const T r = mid + half * g.s[j];
+      const T wt = half * g.jw[j];
+      const T c = (r * r + zp2) / (r * zs * 2.0);
+      const T om = one - mu_of(r);
+      const T f = r * acos_clamped(c) * wt * 2.0;
+      M[0] = M[0] + f;
+      M[1] = M[1] + f * om;
+      M[2] = M[2] + f * om * om;
+    }
+  }
+}
 
 struct ModelGrad {
   double m;
   double d[6];   // dm / d(P, T0, D, depth, u1, u2)
 };
 
-__device__ __forceinline__ double sigmoid(double x) { return 1.0 / (1.0 + exp(-x)); }
-
-// softplus_k(x) and its derivative
-__device__ __forceinline__ void softplus_k(double x, double* v, double* dv) {
-  const double kx = kSoftK * x;
-  if (kx > 30.0) {
-    *v = x + log1p(exp(-kx)) / kSoftK;
-  } else {
-    *v = log1p(exp(kx)) / kSoftK;
-  }
-  *dv = sigmoid(kx);
-}
-
+// Model flux at time t for parameters th, and with kGrad its six derivatives.
 template <bool kGrad>
-__device__ __forceinline__ ModelGrad transit_model(double t, const double* th) {
+__device__ __forceinline__ ModelGrad transit_model(double t, const double* th, const GLTable& g) {
   const double P = th[0], T0 = th[1], D = th[2], depth = th[3], u1 = th[4], u2 = th[5];
-  const double x = t - T0;
-  const double ep = rint(x / P);
-  const double tau = x - ep * P;
-  const double s = 2.0 * tau / D;
-  const double q = 1.0 - s * s;
-  const double B = sigmoid(q / kEdge);
-  double g, dg;
-  softplus_k(q, &g, &dg);
-  // far outside the transit softplus underflows; the floor keeps d(sqrt g) = 0 there
-  const double mu = sqrt(fmax(g, 1e-300));
-  const double om = 1.0 - mu;
-  const double I = 1.0 - u1 * om - u2 * om * om;
-  double g0, dg0;
-  softplus_k(1.0, &g0, &dg0);
-  const double mu0 = sqrt(g0);
-  const double om0 = 1.0 - mu0;
-  const double I0 = 1.0 - u1 * om0 - u2 * om0 * om0;
-  const double shape = B * I / I0;
   ModelGrad r;
-  r.m = 1.0 - depth * shape;
-  if (kGrad) {
-    // d/ds of B*I
-    const double dq = -2.0 * s;
-    const double dB = B * (1.0 - B) * dq / kEdge;
-    const double dmu = dg * dq / (2.0 * mu);
-    const double dI = (u1 + 2.0 * u2 * om) * dmu;
-    const double dm_ds = -depth * (dB * I + B * dI) / I0;
-    const double ds_dtau = 2.0 / D;
-    r.d[0] = dm_ds * ds_dtau * (-ep);           // P
-    r.d[1] = dm_ds * ds_dtau * (-1.0);          // T0
-    r.d[2] = dm_ds * (-s / D);                  // D
-    r.d[3] = -shape;                            // depth
-    // u1, u2 through I and I0
-    const double dI_u1 = -om, dI0_u1 = -om0;
-    const double dI_u2 = -om * om, dI0_u2 = -om0 * om0;
-    r.d[4] = -depth * B * (dI_u1 * I0 - I * dI0_u1) / (I0 * I0);
-    r.d[5] = -depth * B * (dI_u2 * I0 - I * dI0_u2) / (I0 * I0);
+  r.m = 1.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) r.d[k] = 0.0;
+  const double K = 1.0 - u1 / 3.0 - u2 / 6.0;
+  const double dk = depth * K;
+  if (!(dk > 0.0)) return r;
+  const double p = sqrt(dk);
+  const double ang = kPi * D / P;
+  const double sD = sin(ang);
+  const double a = (1.0 + p) / sD;
+  const double x = t - T0;
+  const double q = x / P;
+  const double phi = 2.0 * kPi * (q - rint(q));
+  double sphi, cphi;
+  sincos(phi, &sphi, &cphi);
+  if (cphi < 0.0) return r;                 // the far side of the orbit never occults
+  const double S = fabs(sphi);
+  const double z = a * S;
+  if (!(z < 1.0 + p)) return r;
+  const double norm = kPi * K;
+  if (!kGrad) {
+    double M[3];
+    occultation_moments<double>(z, p, g, M);
+    r.m = 1.0 - (M[0] - u1 * M[1] - u2 * M[2]) / norm;
+    return r;
   }
+  D2 M[3];
+  occultation_moments<D2>(D2{z, 1.0, 0.0}, D2{p, 0.0, 1.0}, g, M);
+  const D2 N = M[0] - M[1] * u1 - M[2] * u2;
+  r.m = 1.0 - N.v / norm;
+  const double lz = N.z / norm, lp = N.p / norm;
+  const double lu1 = (-M[1].v + N.v / (3.0 * K)) / norm;
+  const double lu2 = (-M[2].v + N.v / (6.0 * K)) / norm;
+  // chain rule to the parameters
+  const double cD = cos(ang);
+  const double dp_depth = K / (2.0 * p), dp_u1 = -depth / (6.0 * p), dp_u2 = -depth / (12.0 * p);
+  const double da_p = 1.0 / sD;
+  const double da_D = -(1.0 + p) * cD * (kPi / P) / (sD * sD);
+  const double da_P = (1.0 + p) * cD * (kPi * D / (P * P)) / (sD * sD);
+  const double dS_phi = (sphi > 0.0 ? 1.0 : (sphi < 0.0 ? -1.0 : 0.0)) * cphi;
+  const double dphi_P = -2.0 * kPi * x / (P * P), dphi_T0 = -2.0 * kPi / P;
+  const double dz_P = S * da_P + a * dS_phi * dphi_P;
+  const double dz_T0 = a * dS_phi * dphi_T0;
+  const double dz_D = S * da_D;
+  const double dz_p = S * da_p;
+  r.d[0] = -(lz * dz_P);
+  r.d[1] = -(lz * dz_T0);
+  r.d[2] = -(lz * dz_D);
+  r.d[3] = -((lz * dz_p + lp) * dp_depth);
+  r.d[4] = -((lz * dz_p + lp) * dp_u1 + lu1);
+  r.d[5] = -((lz * dz_p + lp) * dp_u2 + lu2);
   return r;
 }
 
@@ -117,7 +265,7 @@ __global__ void __launch_bounds__(kAdjThreads) model_fwd_kernel(const double* __
                                                                 const double* __restrict__ w,
                                                                 const int64_t* __restrict__ off,
                                                                 const double* __restrict__ params,
-                                                                double* __restrict__ chi2) {
+                                                                double* __restrict__ chi2, const GLTable g) {
   __shared__ double sh[2 * 32 + 2];
   const int c = blockIdx.x;
   double th[6];
@@ -125,7 +273,7 @@ __global__ void __launch_bounds__(kAdjThreads) model_fwd_kernel(const double* __
   for (int k = 0; k < 6; ++k) th[k] = params[6 * c + k];
   double acc[1] = {0.0};
   for (long long i = off[c] + threadIdx.x; i < off[c + 1]; i += blockDim.x) {
-    const ModelGrad r = transit_model<false>(t[i], th);
+    const ModelGrad r = transit_model<false>(t[i], th, g);
     const double res = y[i] - r.m;
     acc[0] += w[i] * res * res;
   }
@@ -139,7 +287,7 @@ __global__ void __launch_bounds__(kAdjThreads) model_bwd_kernel(const double* __
                                                                 const int64_t* __restrict__ off,
                                                                 const double* __restrict__ params,
                                                                 const double* __restrict__ grad_out,
-                                                                double* __restrict__ grad) {
+                                                                double* __restrict__ grad, const GLTable g) {
   __shared__ double sh[7 * 32 + 7];
   const int c = blockIdx.x;
   double th[6];
@@ -147,7 +295,7 @@ __global__ void __launch_bounds__(kAdjThreads) model_bwd_kernel(const double* __
   for (int k = 0; k < 6; ++k) th[k] = params[6 * c + k];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (long long i = off[c] + threadIdx.x; i < off[c + 1]; i += blockDim.x) {
-    const ModelGrad r = transit_model<true>(t[i], th);
+    const ModelGrad r = transit_model<true>(t[i], th, g);
     const double f = -2.0 * w[i] * (y[i] - r.m);
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] += f * r.d[k];
@@ -168,7 +316,7 @@ extern "C" int gtls_model_chi2(gtls_ctx* ctx, const double* t, const double* y, 
     return fail(ctx, GTLS_E_INVALID, "bad arguments to gtls_model_chi2");
   GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
   model_fwd_kernel<<<n_curves, kAdjThreads, 0, static_cast<cudaStream_t>(stream)>>>(t, y, w, curve_off, params,
-                                                                                    chi2_out);
+                                                                                    chi2_out, gl_table());
   ctx->launches += 1;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
   return GTLS_OK;
@@ -182,7 +330,8 @@ extern "C" int gtls_model_chi2_grad(gtls_ctx* ctx, const double* t, const double
     return fail(ctx, GTLS_E_INVALID, "bad arguments to gtls_model_chi2_grad");
   GTLS_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
   model_bwd_kernel<<<n_curves, kAdjThreads, 0, static_cast<cudaStream_t>(stream)>>>(t, y, w, curve_off, params,
-                                                                                    grad_chi2, grad_params);
+                                                                                    grad_chi2, grad_params,
+                                                                                    gl_table());
   ctx->launches += 1;
   GTLS_TRY_CUDA(ctx, cudaGetLastError());
   return GTLS_OK;

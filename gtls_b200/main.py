@@ -10,10 +10,13 @@ Extra keywords: ``precision`` ("fp64" plain FP64 search, default; "fp32" FP32
 chi2 with float-float prefix sums in the main pass and the candidate
 re-search, then an FP64 re-check of the 32 best candidates),
 ``batch_periods`` (periods per duration-union batch; default: the reference's
-free-memory formula, core.py:620-628) and ``distributed`` (shard the main pass
+free-memory formula, core.py:620-628), ``distributed`` (shard the main pass
 over the ranks of the initialised torch.distributed process group, one
 process per GPU: batch-aligned period ranges, chi2 all-gathered; every rank
-returns the same result).
+returns the same result) and ``refine`` (move the best peak's period, T0,
+duration and depth below grid resolution with the adjoint of the
+limb-darkened model chi2; the grid values stay if the chi2 does not
+decrease; both are in ``diagnostics["refinement"]``).
 """
 import warnings
 
@@ -77,9 +80,28 @@ class gtls(object):
          SDE, chi2, self.transitTimes, power, snr, snrPink, snrFit, snrFitPink, raw_power, raw_chi2,
          cand_idx, cand_p, diag) = out
         self.rawDurations = durations
+        if self.refine:
+            self._refine(periods, diag)
         return gtlsResult(self.periods, self.period, self.rawDuration, durationPoints, durations, self.duration,
                           self.Depth, self.bestT0, SDE, chi2, self.transitTimes, power, snr, snrPink, snrFit,
                           snrFitPink, raw_power, raw_chi2, cand_idx, cand_p, diag)
+
+    def _refine(self, periods, diag):
+        """Sub-grid refinement of the best peak (refine=True): the adjoint of
+        the limb-darkened model chi2 from the grid's (period, T0, duration,
+        depth) and the template's limb darkening; the refined values replace
+        the grid's only if the model chi2 decreased.  ``diagnostics
+        ["refinement"]`` keeps both."""
+        from . import refine as R
+        start, scale = R.grid_start(self.period, self.bestT0, self.duration, self.Depth, self.u, periods, self.t)
+        params, chi, chi0, ok = R.refine_peaks([(self.t, self.y, self.dy)], start[None], scale[None],
+                                               device=self.GPUDeviceID)
+        diag["refinement"] = dict(grid=dict(period=self.period, T0=self.bestT0, duration=self.duration,
+                                            depth=self.Depth), params=params[0], chi2=float(chi[0]),
+                                  chi2_grid=float(chi0[0]), improved=bool(ok[0]))
+        if ok[0]:
+            self.period, self.bestT0, self.duration, self.Depth = (float(v) for v in params[0][:4])
+            self.transitTimes = R.refined_transit_times(self.transitTimes, self.bestT0, self.period)
 
     def periodogram(self, **kwargs):
         """The trial periods power() would search (main.py:186-205)."""

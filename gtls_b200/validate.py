@@ -116,6 +116,10 @@ def validate_args(self, kwargs):
     # distributed: shard the search over the ranks of the initialised
     # torch.distributed process group (one process per GPU)
     self.distributed = bool(kwargs.get("distributed", False))
+    # refine: move the best peak below grid resolution with the adjoint of
+    # the limb-darkened model chi2 (the grid result is kept if chi2 does not
+    # decrease)
+    self.refine = bool(kwargs.get("refine", False))
 
     if "b" in kwargs:
         self.b = kwargs.get("b")

@@ -273,11 +273,18 @@ int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t
  * curve_off[c] .. curve_off[c+1]-1, w = 1/dy^2).  params[6c..6c+5] =
  * (P, T0, D, depth, u1, u2) of curve c.  An addition with no counterpart in
  * the reference, used to refine a search peak below grid resolution.
- * Model: tau = (t-T0) - P round((t-T0)/P), s = 2 tau / D,
- * m = 1 - depth B(s) I(s) / I(0), B = sigmoid((1-s^2)/0.05),
- * I = 1 - u1 (1-mu) - u2 (1-mu)^2, mu = sqrt(max(softplus_200(1-s^2), 1e-300)).
- * gtls_model_chi2_grad writes grad_params[6c+k] = grad_chi2[c] * dchi2_c/dparam_k,
- * recomputing the model instead of storing it.
+ * Model: the search's template model, a central (impact parameter 0)
+ * circular-orbit transit of an opaque disk across a star with quadratic limb
+ * darkening I = 1 - u1 (1-mu) - u2 (1-mu)^2: K = 1 - u1/3 - u2/6,
+ * p = sqrt(depth K), a = (1 + p) / sin(pi D / P),
+ * phi = 2 pi ((t-T0)/P - round((t-T0)/P)), z = a |sin phi| (no occultation
+ * when cos phi < 0), m = 1 - (occulted flux at separation z) / (pi K), the
+ * occulted flux integrated over annuli with 96-node Gauss-Legendre
+ * quadrature after r = m + h sin(theta) (the template generator's own
+ * quadrature).  D is the first-to-fourth-contact duration, depth the central
+ * depth.  gtls_model_chi2_grad writes grad_params[6c+k] =
+ * grad_chi2[c] * dchi2_c/dparam_k, the exact derivative of that discrete
+ * formula, recomputing the model instead of storing it.
  */
 int gtls_model_chi2(gtls_ctx* ctx, const double* t, const double* y, const double* w,
                     const int64_t* curve_off, int32_t n_curves, const double* params,

@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference tree (default path below) and the
-CPU build of its kernels (``make -C oracle``):
+Run in a checkout that has the reference tree and the CPU build of its
+kernels (``make -C oracle``); the reference root is the first argument, else
+the REFERENCE_ROOT environment variable:
 
     python tests/golden/make_golden.py [/path/to/reference]
 
@@ -15,6 +16,14 @@ What is recorded, and from which reference code:
 * ``cache.npz``    -- transit.get_cache (src/gputls/transit.py) with its batman
                      light curve replaced by this project's limb-darkening model
                      (batman is a third-party package outside the reference);
+* ``stats.npz``    -- the statistics of the best period: stats.intransit_stats,
+                     stats.snr_stats, stats.pink_noise, stats.all_transit_times,
+                     stats.calcDurationDays and helpers.transit_mask
+                     (src/gputls/stats.py:233-488, helpers.py:62-65), combined
+                     as search_single_periods does (core.py:1427-1499: depth,
+                     T0, duration, transit times, snr, snr_pink, snrFit,
+                     snrFitPink; the snrFit lines are inline in core.py, which
+                     imports cupy, so they are restated here in its order);
 * ``kernels.npz``  -- per-period chi2 and argmin of the reference's CUDA kernels
                      (src/gputls/GPUFun.cu) compiled for the CPU and launched in
                      core.py's order (oracle/ref_replay.py), R64 and R32, for
@@ -159,8 +168,79 @@ def main(ref_root):
         k["case%d_templates" % i] = tm
         k["case%d_maxd" % i] = np.array([maxd])
     np.savez_compressed(os.path.join(HERE, "kernels.npz"), **k)
+    stats_fixture(R)
     print("fixtures written to", HERE)
 
 
+def reference_best_period_stats(R, t, y, period, loc, width, raw_duration, ovs, maxd):
+    """search_single_periods after its chi2 minimum (core.py:1427-1499) with
+    the reference's stats and helpers functions."""
+    st, hp = R["stats"], R["helpers"]
+    tsize = len(t)
+    phase = (t % period) / period                      # foldCPU core.py:16-20
+    rank = np.argsort(phase)
+    best_t, best_f = np.array(t[rank]), y[rank]
+    best_f = np.concatenate((best_f, best_f[:maxd]))
+    k0 = loc % tsize
+    mean = best_f[k0:k0 + width].mean()
+    depth = (1 - mean) * ovs
+    out_tr = np.concatenate((best_f[0:k0], best_f[k0 + width:]))
+    snr_fit = (1 - depth) * (width ** 0.5) / np.std(out_tr)
+    csum = np.cumsum(out_tr)
+    red = np.std((csum[width:] - csum[:-width]) / width)
+    tx = best_t[k0]
+    T0 = tx - int((tx - min(t)) / period) * period - period
+    tt = st.all_transit_times(T0, t, period)
+    snr_fit_pink = (1 - depth) / ((np.std(out_tr) ** 2 / width) + (red ** 2 / len(tt))) ** 0.5
+    dur = st.calcDurationDays(t, period, T0, raw_duration)
+    T0 = T0 + dur / 2
+    tt = np.array(tt) + dur / 2
+    if T0 < min(t):
+        T0 = T0 + period
+    ins = st.intransit_stats(t, y, tt, dur)
+    snr_pt, snr_pink_pt = st.snr_stats(t=t, y=y, period=period, duration=raw_duration, T0=T0, transit_times=tt,
+                                       transit_duration_in_days=dur, per_transit_count=ins[6])
+    f_in = np.concatenate([ins[4], ins[5]])
+    mask = hp.transit_mask(t, period, 2 * raw_duration, T0)
+    ootr = y[~mask]
+    snr = ((1 - np.mean(f_in)) / np.std(ootr)) * len(f_in) ** 0.5
+    snr_pink = np.mean(snr_pink_pt) * (len(tt) ** 0.5)
+    return dict(depth=depth, T0=T0, duration=dur, transit_times=tt, snr=snr, snr_pink=snr_pink, snr_fit=snr_fit,
+                snr_fit_pink=snr_fit_pink, intransit=np.array(ins[:4], dtype=float), per_transit_count=ins[6],
+                transit_depths=ins[7], depth_uncertainties=ins[8], snr_per_transit=snr_pt,
+                snr_pink_per_transit=snr_pink_pt, mask=mask, ootr=ootr)
+
+
+def stats_fixture(R):
+    """stats.npz: three seeded curves, the chi2 minimum of their true period
+    from the oracle, and the reference's statistics of that minimum."""
+    from gtls_b200 import synthetic, template, grid as G, validate as V
+    import tls_oracle as O
+    cases = [synthetic.light_curve_cfg1(seed=4, n=5000, period=1.9, depth=2500e-6)[:2] + (None, 1.9),
+             synthetic.small_curve(seed=8, n=1500, span=6.0, dy=True) + (1.7,),
+             synthetic.light_curve_cfg1(seed=6, n=14000, period=4.4, depth=800e-6)[:2] + (None, 4.4)]
+    f = {}
+    for i, (t, y, dy, period) in enumerate(cases):
+        t, y, dy = V.validate_inputs(t, y, dy)
+        P = np.sort(O.period_grid(1, 1, t.max() - t.min()))
+        durs = G.duration_grid(P, shortest=1 / len(t))
+        mw = int(np.max(durs) * len(y))
+        mw += mw % 2
+        ov, lc = template.get_cache(durs, mw, 12.9, 0.03, 23.1, 89.21, 0, 90, [0.4804, 0.1867], "quadratic")
+        widths, os_, dd, tm, maxd = template.device_templates(lc, ov)
+        fin = O.single_period(O.NumpyBackend(), period, t, y, dy, widths, tm, os_, dd, maxd, 1e-5)
+        loc, width, raw = fin["loc"], fin["width"], fin["raw_duration"]
+        ovs = float(os_[int(np.nonzero(widths == width)[0][0])])
+        ref = reference_best_period_stats(R, t, y, period, loc, width, raw, ovs, int(maxd))
+        f["case%d_inputs" % i] = np.array([period, loc, width, raw, ovs, maxd], dtype=float)
+        f["case%d_t" % i] = t
+        f["case%d_y" % i] = y
+        ootr = ref.pop("ootr")
+        f["case%d_pink" % i] = np.array([R["stats"].pink_noise(ootr, w) for w in (1, 5, 37)])
+        for k, v in ref.items():
+            f["case%d_%s" % (i, k)] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, "stats.npz"), **f)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT", "/root/reference"))

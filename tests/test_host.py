@@ -302,3 +302,35 @@ def test_template_cache_equals_the_per_duration_loop():
         assert len(lc) == len(lc_ref)
         for a, b in zip(lc, lc_ref):
             np.testing.assert_array_equal(a, b)
+
+
+def test_best_period_statistics_match_reference():
+    """Depth, T0, duration, transit times, snr, snr_pink, snrFit and
+    snrFitPink of a chi2 minimum (core.finish_stats) and the statistics
+    functions one by one, against the reference's own stats.py/helpers.py
+    (golden stats.npz).  pink_noise runs in O(N) from prefix sums here, so
+    the pink-noise figures carry a 1e-12 bar; the rest is the same arithmetic."""
+    from gtls_b200 import core, stats
+    f = golden("stats")
+    for i in range(3):
+        period, loc, width, raw, ovs, maxd = f["case%d_inputs" % i]
+        t, y = f["case%d_t" % i], f["case%d_y" % i]
+        g = {k[len("case%d_" % i):]: f[k] for k in f.files if k.startswith("case%d_" % i)}
+        out = core.finish_stats(t, y, period, int(loc), int(width), raw, ovs, int(maxd))
+        for k in ("depth", "T0", "duration", "snr", "snr_fit", "snr_fit_pink"):
+            np.testing.assert_allclose(out[k], g[k], rtol=1e-13, err_msg=k)
+        np.testing.assert_allclose(out["snr_pink"], g["snr_pink"], rtol=1e-12)
+        np.testing.assert_allclose(out["transit_times"], g["transit_times"], rtol=1e-15)
+        tt, dur = g["transit_times"], float(g["duration"])
+        ins = stats.intransit_stats(t, y, tt, dur)
+        np.testing.assert_allclose(np.array(ins[:4], dtype=float), g["intransit"], rtol=1e-13)
+        np.testing.assert_array_equal(ins[6], g["per_transit_count"])
+        np.testing.assert_allclose(ins[7], g["transit_depths"], rtol=1e-15)
+        np.testing.assert_allclose(ins[8], g["depth_uncertainties"], rtol=1e-13)
+        snr_pt, snr_pink_pt = stats.snr_stats(t, y, period, raw, float(g["T0"]), tt, dur, ins[6])
+        np.testing.assert_allclose(snr_pt, g["snr_per_transit"], rtol=1e-13)
+        np.testing.assert_allclose(snr_pink_pt, g["snr_pink_per_transit"], rtol=1e-12)
+        mask = stats.transit_mask(t, period, 2 * raw, float(g["T0"]))
+        np.testing.assert_array_equal(mask, g["mask"])
+        pink = [stats.pink_noise(y[~mask], w) for w in (1, 5, 37)]
+        np.testing.assert_allclose(pink, g["pink"], rtol=1e-12, atol=1e-300)
