@@ -107,6 +107,18 @@ class CurveOnDevice:
             max_width=self.maxd,
         )
 
+    def on_device(self, device):
+        """The same curve and tables on another device (self for the same one)."""
+        if device == self.device:
+            return self
+        import copy
+        other = copy.copy(self)
+        other.device = device
+        other.dev = self.torch.device("cuda:%d" % device)
+        other.curve = {k: (v.to(other.dev) if hasattr(v, "to") else v) for k, v in self.curve.items()}
+        other.tables = {k: (v.to(other.dev) if hasattr(v, "to") else v) for k, v in self.tables.items()}
+        return other
+
     def search(self, periods, depth_min, skip_point, batch, pass_, precision, want_loc=False, timing=None,
                tables=None, flags=0):
         torch = self.torch
@@ -192,26 +204,29 @@ def _candidates(power_dev, mask_dev, periods_dev, torch):
 
 def search_multi_periods(periods, t, y, dy, transit_depth_min, lc_arr, lc_cache_overview, T0_fit_margin,
                          oversampling_factor, verbose=False, GPUDeviceID=0, fast=False, precision="fp64",
-                         batch_periods=None, distributed=False):
+                         batch_periods=None, distributed=False, devices=None):
     """GPU counterpart of core.search_multi_periods (core.py:568-999).
 
     Returns the reference's 19 values (periods, period, rawDuration,
     durationPoints, duration, depth, T0, SDE, chi2, transitTimes, power, snr,
     snrPink, snrFit, snrFitPink, raw_power, raw_chi2, candidate indices,
     candidate periods) plus a dict of diagnostics, or (periods, power) when
-    ``fast``.
+    ``fast``.  ``devices``: more than one CUDA device ids shard the main pass
+    over them in this process (the reference's ``GPUDeviceIDs``); the rest
+    runs on ``GPUDeviceID``.
     """
     import torch
     periods = np.sort(np.asarray(periods, dtype=np.float64))
     cur = CurveOnDevice(t, y, dy, lc_arr, lc_cache_overview, device=GPUDeviceID)
     periods_dev = _h2d(torch, periods, cur.dev)
     return run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_margin, oversampling_factor,
-                      fast=fast, precision=precision, batch_periods=batch_periods, distributed=distributed)
+                      fast=fast, precision=precision, batch_periods=batch_periods, distributed=distributed,
+                      devices=devices)
 
 
 def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_margin, oversampling_factor,
                fast=False, precision="fp64", batch_periods=None, timing=None, distributed=False, group=None,
-               phases=None):
+               phases=None, devices=None):
     """The search on a curve already resident on the device (see search_multi_periods).
 
     ``periods``: sorted host array, ``periods_dev`` the same on the device.
@@ -251,6 +266,14 @@ def run_search(cur, periods, periods_dev, t, y, dy, transit_depth_min, T0_fit_ma
 
         chi2_dev = shard.sharded_period_pass(len(periods), S, main_pass, group=group,
                                              device=dev if nccl else None).to(dev)
+    elif devices is not None and len(devices) > 1:
+        curves = {int(d): cur.on_device(int(d)) for d in devices}
+
+        def main_pass_on(d, p0, p1):
+            c, _ = curves[d].search(periods[p0:p1], transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision)
+            return _d2h(c)
+
+        chi2_dev = _h2d(torch, shard.multi_device_period_pass(len(periods), S, list(devices), main_pass_on), dev)
     else:
         chi2_dev, _ = cur.search(periods_dev, transit_depth_min, skip, S, _lib.GTLS_PASS_MAIN, precision,
                                  timing=timing)

@@ -240,10 +240,15 @@ __device__ __forceinline__ int phase_bin(double ph, int nb_log2) {
 // index (the order of a stable argsort).  The 32-bit keys are the in-bucket
 // fractions rounded to float, which preserves every strict inequality; equal
 // keys are decided on the exact FP64 phases, recomputed.
-__device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __restrict__ t, double P) {
+// Slot index words hold the sample index, and for curves of at most
+// kPackedMaxN samples also the bucket in the bits above it (the same for two
+// slots of one bucket, so comparing whole words compares the indices).
+constexpr int kPackedShift = 17;
+constexpr int kPackedMaxN = 1 << kPackedShift;
+__device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __restrict__ t, double P, unsigned imask) {
   const float fa = __uint_as_float(a.x), fb = __uint_as_float(b.x);
   if (fa != fb) return fa < fb;
-  const double pa = fold_phase(t[a.y], P), pb = fold_phase(t[b.y], P);
+  const double pa = fold_phase(t[a.y & imask], P), pb = fold_phase(t[b.y & imask], P);
   if (pa != pb) return pa < pb;
   return a.y < b.y;
 }
@@ -255,7 +260,7 @@ __device__ __forceinline__ bool slot_less(uint2 a, uint2 b, const double* __rest
 // otherwise fall on single threads.
 template <typename Emit>
 __device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot, int s, int e,
-                                                 const double* __restrict__ t, double P, Emit emit) {
+                                                 const double* __restrict__ t, double P, unsigned imask, Emit emit) {
   const int lane = threadIdx.x & 31;
   for (int j0 = s; j0 < e; j0 += 32) {
     const int j = j0 + lane;
@@ -268,10 +273,10 @@ __device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot,
         uint2 o;
         o.x = __shfl_sync(0xffffffffu, oth.x, q);
         o.y = __shfl_sync(0xffffffffu, oth.y, q);
-        if (o.y != mine.y && slot_less(o, mine, t, P)) ++r;
+        if (o.y != mine.y && slot_less(o, mine, t, P, imask)) ++r;
       }
     }
-    if (j < e) emit(s + r, (int)mine.y);
+    if (j < e) emit(s + r, (int)(mine.y & imask));
   }
 }
 
@@ -301,6 +306,8 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   const int maxd = C.maxd;
   const int nb_log2 = C.nb_log2;
   const int nb = 1 << nb_log2;
+  const bool packed = n <= kPackedMaxN && nb_log2 <= 32 - kPackedShift;
+  const unsigned imask = packed ? (unsigned)(kPackedMaxN - 1) : 0xffffffffu;
   const double P = C.periods[R.pidx0 + local];
   const int M = C.M;
   const int Mrec = C.Mrec;
@@ -348,7 +355,7 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
         const int b = phase_bin(ph, nb_log2);
         const int s = atomicAdd(&hist[b], 1);
         const float f = (float)(ldexp(ph, nb_log2) - (double)b);
-        slot[s] = make_uint2(__float_as_uint(f), (unsigned)i);
+        slot[s] = make_uint2(__float_as_uint(f), (unsigned)i | (packed ? (unsigned)b << kPackedShift : 0u));
       }
     }
   }
@@ -391,33 +398,40 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   if (warp_ranked)
     for (int q = (int)(threadIdx.x >> 5); q < nbig; q += (int)(blockDim.x >> 5)) {
       const int b = big[q];
-      rank_bucket_warp(slot, b == 0 ? 0 : hist[b - 1], hist[b], t, P, emit);
+      rank_bucket_warp(slot, b == 0 ? 0 : hist[b - 1], hist[b], t, P, imask, emit);
     }
   //     (c) every other entry is ranked by its own thread: coalesced over the
-  //         slots, its bucket found by binary search of the bucket ends (the
-  //         emitted positions are then close to the slot index, so the
-  //         record writes stay nearly coalesced).
+  //         slots, its bucket read from the slot word (packed) or found by
+  //         binary search of the bucket ends (the emitted positions are then
+  //         close to the slot index, so the record writes stay nearly
+  //         coalesced).
   for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int j = i0 + u * blockDim.x;
       if (j < n) {
-        int lo = 0, hi = nb - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi) >> 1;
-          if (hist[mid] > j) hi = mid;
-          else lo = mid + 1;
+        const uint2 sj = slot[j];
+        int lo;
+        if (packed) {
+          lo = (int)(sj.y >> kPackedShift);
+        } else {
+          lo = 0;
+          int hi = nb - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (hist[mid] > j) hi = mid;
+            else lo = mid + 1;
+          }
         }
         const int s = lo == 0 ? 0 : hist[lo - 1];
         const int e = hist[lo];
-        const uint2 sj = slot[j];
         if (e - s == 1) {
-          emit(j, (int)sj.y);
+          emit(j, (int)(sj.y & imask));
         } else if (e - s <= kSmallBucket || !warp_ranked) {
           int r = 0;
           for (int m = s; m < e; ++m)
-            if (m != j) r += slot_less(slot[m], sj, t, P);
-          emit(s + r, (int)sj.y);
+            if (m != j) r += slot_less(slot[m], sj, t, P, imask);
+          emit(s + r, (int)(sj.y & imask));
         }
       }
     }

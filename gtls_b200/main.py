@@ -3,9 +3,11 @@
 Same constructor, same ``power()`` keywords (constants.VALID_PARAMETERS) and
 the same return: a ``gtlsResult`` or, with ``fast=True``, ``(periods, power)``.
 The search runs on one GPU (``GPUDeviceID``); ``GPUDeviceIDs`` with more than
-one entry is accepted and runs on the first device: the reference's own
-multi-GPU mode (worker processes per GPU) is replaced by ``distributed``
-below, with one process per GPU started by torchrun.
+one entry shards the main pass over those devices in this process, as the
+reference's multi-GPU mode does with a worker process per GPU (contiguous,
+batch-aligned period ranges, one host thread per device; every chi2 value is
+the unsharded one), and runs the rest on the first of them.  ``distributed``
+(below) does the same with one process per GPU started by torchrun.
 Extra keywords: ``precision`` ("fp64" plain FP64 search, default; "fp32" FP32
 chi2 with float-float prefix sums in the main pass and the candidate
 re-search, then an FP64 re-check of the 32 best candidates),
@@ -18,8 +20,6 @@ duration and depth below grid resolution with the adjoint of the
 limb-darkened model chi2; the grid values stay if the chi2 does not
 decrease; both are in ``diagnostics["refinement"]``).
 """
-import warnings
-
 import numpy as np
 
 from . import constants, core
@@ -49,10 +49,10 @@ class gtls(object):
     def power(self, **kwargs):
         """Run the search; see the module docstring for the keywords."""
         self, kwargs = validate_args(self, kwargs)
+        devices = None
         if self.GPUDeviceIDs is not None and len(self.GPUDeviceIDs) > 0:
-            if len(self.GPUDeviceIDs) > 1:
-                warnings.warn("GPUDeviceIDs: the search runs on device %d only" % self.GPUDeviceIDs[0])
-            self.GPUDeviceID = self.GPUDeviceIDs[0]
+            devices = [int(d) for d in self.GPUDeviceIDs]
+            self.GPUDeviceID = devices[0]
         if self.verbose:
             print(constants.BANNER)
         periods = self._grids()
@@ -73,7 +73,7 @@ class gtls(object):
             lc_arr=self.lc_arr, lc_cache_overview=self.lc_cache_overview, T0_fit_margin=self.T0_fit_margin,
             oversampling_factor=self.oversampling_factor, verbose=self.verbose, GPUDeviceID=self.GPUDeviceID,
             fast=self.fast, precision=self.precision, batch_periods=self.batch_periods,
-            distributed=self.distributed)
+            distributed=self.distributed, devices=devices)
         if self.fast:
             return out
         (self.periods, self.period, self.rawDuration, durationPoints, self.duration, self.Depth, self.bestT0,

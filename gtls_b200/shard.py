@@ -125,3 +125,38 @@ def sharded_curves(costs, search_subset, group=None):
         for i, res in pairs:
             out[i] = res
     return out
+
+
+def multi_device_period_pass(n_periods, batch, devices, main_pass):
+    """The reference's in-process multi-GPU mode (``power(GPUDeviceIDs=[...])``,
+    core.py:318-564: contiguous period ranges per GPU, concatenated): the
+    period list is cut into one batch-aligned range per entry of ``devices``
+    (so every chi2 value is the unsharded one) and ``main_pass(device, p0,
+    p1)`` (a host float64 array) runs for each, one host thread per distinct
+    device so that the devices work at the same time (ranges of a repeated
+    device run one after the other on it).  Returns the concatenated host
+    array."""
+    import threading
+    ranges = aligned_ranges(n_periods, batch, len(devices))
+    out = [None] * len(devices)
+    errors = []
+    by_device = {}
+    for i, d in enumerate(devices):
+        by_device.setdefault(int(d), []).append(i)
+
+    def work(idx):
+        try:
+            for i in idx:
+                a, b = ranges[i]
+                out[i] = main_pass(int(devices[i]), a, b) if b > a else np.zeros(0)
+        except Exception as e:   # re-raised on the calling thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(idx,)) for idx in by_device.values()]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    return np.concatenate([np.asarray(o, dtype=np.float64) for o in out])

@@ -120,7 +120,8 @@ def test_power_refine_moves_the_peak_below_grid_resolution(cuda):
     the injected ones than the grid's, the model chi2 decreased, and the grid
     result stays available; gtls_batch(...).power(refine=True) refines every
     curve in one batched run and agrees with the single-curve refinement."""
-    from gtls_b200 import gtls, gtls_batch
+    from gtls_b200 import gtls
+    from gtls_b200.batch import gtls_batch
     t, y, _, truth = synthetic.light_curve_cfg1(seed=5, n=12000, period=2.71, depth=3000e-6, noise=5e-4)
     res = gtls(t, y, verbose=False).power(period_min=0.5, period_max=10.0, refine=True)
     ref = res.diagnostics["refinement"]

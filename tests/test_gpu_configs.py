@@ -15,6 +15,11 @@
   against the same reference kernels: identical argmin locations, chi2
   within 1e-9; and the fold ordering of 16 periods equal to NumPy's stable
   argsort of the FP64 phases.
+* The reference's own call on the TESS sector-58 2-minute light curve it
+  bundles (test1.py:86-150, columns in the golden fixture tess_s58.npz):
+  cleaned, normalised by the mean flux and searched with
+  ``power(periods=np.linspace(1, 14, 10000))``; the script's wotan detrending
+  is left out (wotan is not installed).  Same bars as the 19,728-sample case.
 * The FP32-compensated form of the 19,728-sample search on three seeds of
   the mixed-precision workload (depth log-U(100, 2000) ppm, P log-U(1, 500) d)
   against the FP64 oracle: identical best period index and duration, SDE
@@ -125,5 +130,23 @@ def test_cfg3_fp32_form_agrees_with_the_fp64_oracle(cuda, seed):
     res = model.power(period_min=0.5, period_max=13.7, oversampling_factor=3, precision="fp32")
     ref = _oracle_search(model, res)
     _assert_same_search(res, ref, rtol_chi2=RTOL32, rtol_sde=1e-4)
+    np.testing.assert_allclose([res.depth, res.T0, res.duration], [ref["depth"], ref["T0"], ref["duration"]],
+                               rtol=RTOL64)
+
+
+def test_tess_sector58_reference_call_matches_the_reference_flow(cuda):
+    from conftest import golden
+    from gtls_b200 import gtls, validate as V
+    f = golden("tess_s58")
+    t, y, dy = V.cleaned_array(f["time"], f["pdcsap_flux"], f["pdcsap_flux_err"])
+    y = y / np.nanmean(y)
+    model = gtls(t, y, dy, verbose=False)
+    res = model.power(periods=np.linspace(1, 14, 10000))
+    assert len(model.t) > 15000
+    ref = _oracle_search(model, res)
+    _assert_same_search(res, ref)
+    assert res.diagnostics["loc"] == ref["loc"]
+    assert list(res.possiblePeriodsIndices) == list(ref["candidates"])
+    np.testing.assert_allclose(res.diagnostics["chi2_main"], ref["chi2_main"], rtol=RTOL64)
     np.testing.assert_allclose([res.depth, res.T0, res.duration], [ref["depth"], ref["T0"], ref["duration"]],
                                rtol=RTOL64)

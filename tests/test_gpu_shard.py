@@ -71,3 +71,17 @@ def test_sharded_search_equals_unsharded(cuda):
     np.testing.assert_array_equal(s[0], want)
     np.testing.assert_array_equal(b[0], b[1])
     np.testing.assert_array_equal(b[0], np.array([[x.period, x.SDE, x.depth, x.T0] for x in refb]))
+
+
+@pytest.mark.gpu
+def test_power_with_several_device_ids_equals_one_device(cuda):
+    """power(GPUDeviceIDs=[0, 0, 0]): the main pass in three batch-aligned
+    ranges (on a one-GPU machine all on device 0, one after the other) gives
+    exactly the single-device result."""
+    from gtls_b200 import gtls
+    from conftest import search_inputs
+    s = search_inputs(seed=31, n=1500, span=6.0)
+    one = gtls(s["t"], s["y"], verbose=False).power(periods=s["periods"], batch_periods=7)
+    three = gtls(s["t"], s["y"], verbose=False).power(periods=s["periods"], batch_periods=7, GPUDeviceIDs=[0, 0, 0])
+    np.testing.assert_array_equal(three.diagnostics["chi2_main"], one.diagnostics["chi2_main"])
+    assert three.period == one.period and three.SDE == one.SDE

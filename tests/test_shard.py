@@ -118,3 +118,25 @@ def test_sharded_curves_cover_every_curve_once():
     np.testing.assert_array_equal(c0[:, 1], 10.0 * np.arange(11))
     assert sorted(np.concatenate([s0, s1]).tolist()) == list(range(11))
     assert len(s0) > 0 and len(s1) > 0
+
+
+def test_multi_device_period_pass_concatenates_aligned_ranges_in_order():
+    """GPUDeviceIDs in one process: one batch-aligned range per listed device,
+    ranges of a repeated device run one after the other on its thread, and
+    the chi2 segments come back concatenated in period order."""
+    import threading
+    from gtls_b200 import shard
+    calls = []
+    lock = threading.Lock()
+
+    def main_pass(device, p0, p1):
+        with lock:
+            calls.append((device, p0, p1))
+        return np.arange(p0, p1, dtype=np.float64) * 10 + device
+
+    out = shard.multi_device_period_pass(103, 10, [0, 1, 0, 2], main_pass)
+    ranges = shard.aligned_ranges(103, 10, 4)
+    expect = np.concatenate([np.arange(a, b) * 10.0 + d for (a, b), d in zip(ranges, [0, 1, 0, 2])])
+    np.testing.assert_array_equal(out, expect)
+    assert sorted(calls) == sorted((d, a, b) for (a, b), d in zip(ranges, [0, 1, 0, 2]) if b > a)
+    assert all(a % 10 == 0 for a, _ in ranges)
