@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--chunk-mb", type=int, default=0,
                     help="per-chunk scratch budget of the searches in MiB (default: the library's 8 GiB)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched FP32 vs per-curve FP64 comparison on a sample of the 4,096-curve set")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the leg that times the reference's own kernels on the same GPU")
     ap.add_argument("--max-periods", type=int, default=0,
@@ -286,6 +288,53 @@ def ref_gpu_leg(cur, t, y, dy, lc, ov, periods, batch, ours_main_s, device, n_sa
             "main_pass_speedup": main_s / ours_main_s,
             "r32_vs_ours_fp64": {"periods": total, "same_argmin_location": same / max(total, 1),
                                  "max_rel_chi2_difference": max(rel) if rel else None}}
+
+
+def batched_headline(device, n_curves=16):
+    """The metric's comparison on a sample of the 4,096-curve batched set
+    (every 4096/n_curves-th curve): one gtls_batch(...).power() call in the
+    FP32-compensated form against gtls(...).power(precision="fp64") per curve
+    with the same duration-union batch sizes, both end to end from host
+    arrays (wall clock, after one untimed call of each), with the agreement
+    of best period index and SDE; the sample's share of the set's work gives
+    the extrapolated time of all 4,096 curves."""
+    import torch
+    from gtls_b200 import gtls, synthetic
+    from gtls_b200.batch import gtls_batch, prepare_curve
+    from gtls_b200.validate import validate_args
+    import types
+    specs, idx, total_work = cfg4_sample(n_curves)
+    curves = [synthetic.light_curve_cfg4(specs, int(i))[:2] for i in idx]
+    opts = types.SimpleNamespace()
+    validate_args(opts, dict(use_threads=1, GPUDeviceID=device))
+    work = float(sum(len(c[0]) * len(prepare_curve(c[0], c[1], None, opts, device=device)["periods"])
+                     for c in curves))
+    kw = dict(use_threads=1, GPUDeviceID=device, keep_spectra=False)
+    out = gtls_batch(curves).power(precision="fp32", **kw)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    out = gtls_batch(curves).power(precision="fp32", **kw)
+    torch.cuda.synchronize()
+    b_s = time.perf_counter() - a
+    S = [int(o.batch_periods) for o in out]
+    gtls(curves[0][0], curves[0][1], verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device,
+                                                         batch_periods=S[0])
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    r64 = [gtls(t, y, verbose=False).power(precision="fp64", use_threads=1, GPUDeviceID=device, batch_periods=s)
+           for (t, y), s in zip(curves, S)]
+    torch.cuda.synchronize()
+    p_s = time.perf_counter() - a
+    same = [o.period_index == r.diagnostics["period_index"] for o, r in zip(out, r64)]
+    sde = [abs(o.SDE / r.SDE - 1) for o, r in zip(out, r64)]
+    return {"what": "batched FP32-compensated search (one gtls_batch call) vs plain FP64 per-curve searches "
+                    "(gtls(...).power(precision='fp64') each, same duration-union batch sizes) on every %d-th curve "
+                    "of the 4,096-curve set, end to end from host arrays, wall clock" % (4096 // n_curves),
+            "curves": len(idx), "work_fraction_of_4096_set": work / total_work,
+            "batched_fp32_curves_per_s": len(idx) / b_s, "per_curve_fp64_curves_per_s": len(idx) / p_s,
+            "speedup": p_s / b_s, "best_index_agreement": float(np.mean(same)), "sde_max_rel_diff": float(max(sde)),
+            "full_set_seconds_batched_estimate": b_s * total_work / work,
+            "full_set_seconds_per_curve_fp64_estimate": p_s * total_work / work}
 
 
 def bench_refine(args):
@@ -901,6 +950,8 @@ def main():
     }
     if rank == 0:
         line["clocks"] = clk.summary()
+        if not args.no_batched and world == 1:
+            line["batched"] = batched_headline(device)
         if not args.no_ref_gpu and world == 1:
             main_s = sum(statistics.mean(tm[k] for tm in timings)
                          for k in ("setup_ms", "prepare_ms", "chi2_ms", "finish_ms")) / 1000.0

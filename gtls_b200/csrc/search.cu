@@ -61,6 +61,14 @@ constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset
 // covered by groups of kR consecutive starts (each beginning at the first
 // uncovered start that passes), and only those groups are correlated.
 constexpr int kWin = 4 * kR;
+// All-starts pass, lane-path task of a width of at least kLaneGateMinW: a
+// window of 32 * kLaneG groups of kR consecutive starts; the groups whose
+// starts all fail the depth test are dropped and the others are dealt out to
+// the lanes round by round.  (For shorter widths, and for the main pass's
+// lane-path widths, measured: a group's sums cost about what its depth tests
+// do, and the task is the plain 32 groups.)
+constexpr int kLaneG = 4;
+constexpr int kLaneGateMinW = 64;
 // Zeroed records after each shared-memory tile: a skip-1 group whose kR
 // starts all lie in the tile reads at most kR - 2 records past it (only ever
 // against zero template entries), so those groups need no clamping.
@@ -696,7 +704,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
         const int sk = skips[d];
         const int jlo = (k0 + sk - 1) / sk, jhi = (k1 + sk - 1) / sk;
         const int nj = max(0, jhi - jlo);
-        nt = (sk >= kSplitMinSkip) ? (nj + kWin - 1) / kWin : (nj + 32 * kR - 1) / (32 * kR);
+        const int wd = C.widths[d];
+        nt = (sk >= kSplitMinSkip) ? (nj + kWin - 1) / kWin
+             : (kAllStarts && wd >= kLaneGateMinW ? (nj + 32 * kR * kLaneG - 1) / (32 * kR * kLaneG)
+                                    : (nj + 32 * kR - 1) / (32 * kR));
       }
       int inc = nt;
 #pragma unroll
@@ -836,6 +847,91 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
             eval_start<Real>(best, pre, k, w, inv_w, os, mine, C, a.depth_min, ebase, sentinel, locb + k);
           }
         }
+      }
+    } else if (kAllStarts && w >= kLaneGateMinW) {
+      // lanes own groups of kR consecutive starts.  (1) the depth test of the
+      // window's groups, kLaneG per lane (a start that fails it takes the value
+      // n here); (2) the groups with a passing start, dealt out 32 at a time
+      const int g0 = sub * 32 * kLaneG;
+      unsigned masks[kLaneG];
+      int total = 0;
+#pragma unroll
+      for (int i = 0; i < kLaneG; ++i) {
+        const int jb = jlo + (g0 + 32 * i + lane) * kR;
+        bool any = false;
+        if (jb < jhi) {
+          Pv p0[kR], pw[kR];
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const int k = min(jb + r, jhi - 1) * s;
+            p0[r] = pre[k];
+            pw[r] = pre[k + w];
+          }
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            if (jb + r < jhi) {
+              const bool on = (double)window_mean_of(pw[r], p0[r], inv_w) > a.depth_min;
+              any |= on;
+              if (!on) best_update(best, sentinel, locb + (long long)(jb + r) * s);
+            }
+          }
+        }
+        masks[i] = __ballot_sync(0xffffffffu, any);
+        total += __popc(masks[i]);
+      }
+      for (int q0 = 0; q0 < total; q0 += 32) {
+        const int q = q0 + lane;
+        int jb = jhi;   // no group for lanes past the last one
+        if (q < total) {
+          int before = 0;
+#pragma unroll
+          for (int i = 0; i < kLaneG; ++i) {
+            const int c = __popc(masks[i]);
+            if (q >= before && q < before + c) jb = jlo + (g0 + 32 * i + (int)__fns(masks[i], 0, q - before + 1)) * kR;
+            before += c;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
+        if (jb < jhi) {
+          if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
+            correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
+          } else {
+            for (int rho = 0; rho < s; ++rho)
+              correlate<Real, kTwoLevel>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+          }
+          Pv p0[kR], pw[kR];
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const int k = min(jb + r, jhi - 1) * s;
+            p0[r] = pre[k];
+            pw[r] = pre[k + w];
+          }
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const int j = jb + r;
+            if (j < jhi) {
+              const int k = j * s;
+              eval_mean<Real>(best, window_mean_of(pw[r], p0[r], inv_w), os, acc[r].x, acc[r].y, a.depth_min, ebase,
+                              sentinel, locb + k);
+            }
+          }
+        }
+        if (count_work) {
+          const unsigned ng = __popc(__ballot_sync(0xffffffffu, jb < jhi));
+          if (lane == 0) atomicAdd(&work_sm[1], (unsigned long long)ng * kR * 2ULL * (unsigned)(Qr * s));
+        }
+      }
+      if (count_work) {
+        // starts passing the depth test, counted from the prefix values again
+        unsigned nact = 0;
+        for (int i = 0; i < kLaneG; ++i) {
+          const int jb = jlo + (g0 + 32 * i + lane) * kR;
+          for (int r = 0; r < kR && jb + r < jhi; ++r)
+            nact += (double)window_mean(pre, (jb + r) * s, w, inv_w) > a.depth_min;
+        }
+        nact = __reduce_add_sync(0xffffffffu, nact);
+        if (lane == 0) atomicAdd(&work_sm[0], (unsigned long long)nact * 2ULL * (unsigned)w);
       }
     } else {
 #pragma unroll
