@@ -307,8 +307,8 @@ def batched_headline(device, n_curves=16):
     curves = [synthetic.light_curve_cfg4(specs, int(i))[:2] for i in idx]
     opts = types.SimpleNamespace()
     validate_args(opts, dict(use_threads=1, GPUDeviceID=device))
-    work = float(sum(len(c[0]) * len(prepare_curve(c[0], c[1], None, opts, device=device)["periods"])
-                     for c in curves))
+    work = float(sum(len(c[0]) * len(prepare_curve(c[0], c[1], None, opts, device=device,
+                                                   templates="device")["periods"]) for c in curves))
     kw = dict(use_threads=1, GPUDeviceID=device, keep_spectra=False)
     out = gtls_batch(curves).power(precision="fp32", **kw)
     torch.cuda.synchronize()
@@ -565,7 +565,7 @@ def bench_batch(args):
         return cfg4_once(args, curves, idx, specs, total_work, device)
     opts = types.SimpleNamespace()
     validate_args(opts, dict(precision=args.precision, use_threads=1, GPUDeviceID=device))
-    prepared = [batch.prepare_curve(t, y, None, opts, device=device) for (t, y) in curves]
+    prepared = [batch.prepare_curve(t, y, None, opts, device=device, templates="device") for (t, y) in curves]
     cs = batch.CurveSetOnDevice(prepared, device=device)
     from gtls_b200 import tune
     tuning = fixed_or_tuned(args, lambda: tune.tune_curve_set(cs, args.precision), device)

@@ -130,6 +130,27 @@ class BatchDesc(ctypes.Structure):
     ]
 
 
+class TemplateDesc(ctypes.Structure):
+    """Mirror of ``gtls_template_desc``."""
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("n_curves", ctypes.c_int32),
+        ("per", ctypes.c_double),
+        ("rp", ctypes.c_double),
+        ("a", ctypes.c_double),
+        ("inc", ctypes.c_double),
+        ("u1", ctypes.c_double),
+        ("u2", ctypes.c_double),
+        ("samples", ctypes.c_void_p),
+        ("row_off", ctypes.c_void_p),
+        ("widths", ctypes.c_void_p),
+        ("tmpl_off", ctypes.c_void_p),
+        ("row_len", ctypes.c_void_p),
+        ("overshoot", ctypes.c_void_p),
+        ("templates", ctypes.c_void_p),
+    ]
+
+
 EXPORTS = {
     "gtls_ctx_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "gtls_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
@@ -149,6 +170,7 @@ EXPORTS = {
     "gtls_fold_order": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
                          ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "gtls_search_batch": ([ctypes.c_void_p, ctypes.POINTER(BatchDesc), ctypes.c_void_p], ctypes.c_int),
+    "gtls_template_cache": ([ctypes.c_void_p, ctypes.POINTER(TemplateDesc), ctypes.c_void_p], ctypes.c_int),
     "gtls_spectra": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p], ctypes.c_int),
@@ -290,6 +312,27 @@ def fold_order(t, periods, device=0):
                                 _stream(torch, device))
     _check(rc, ctx, "gtls_fold_order")
     return out
+
+
+def template_cache(planet, samples, row_off, widths, tmpl_off, row_len, overshoot, templates, device=0):
+    """gtls_template_cache: fill the device tensors ``overshoot`` [rows] and
+    ``templates`` with the template tables of every curve.  ``planet`` =
+    (per, rp, a, inc, u1, u2); the other arguments are host arrays (see the
+    C header)."""
+    torch = _torch()
+    ctx = context(device)
+    keep = [np.ascontiguousarray(samples, dtype=np.int32), np.ascontiguousarray(row_off, dtype=np.int64),
+            np.ascontiguousarray(widths, dtype=np.int32), np.ascontiguousarray(tmpl_off, dtype=np.int64),
+            np.ascontiguousarray(row_len, dtype=np.int32)]
+    d = TemplateDesc()
+    d.abi_version = ABI_VERSION
+    d.n_curves = len(keep[0])
+    d.per, d.rp, d.a, d.inc, d.u1, d.u2 = (float(v) for v in planet)
+    d.samples, d.row_off, d.widths, d.tmpl_off, d.row_len = (a.ctypes.data for a in keep)
+    d.overshoot = overshoot.data_ptr()
+    d.templates = templates.data_ptr()
+    rc = load().gtls_template_cache(ctx, ctypes.byref(d), _stream(torch, device))
+    _check(rc, ctx, "gtls_template_cache")
 
 
 def set_tuning(tile_cap_fp32=0, tile_cap_fp64=0, bucket_shift=0, records_global=0, device=0):

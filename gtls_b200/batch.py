@@ -53,18 +53,35 @@ class CurveSetOnDevice:
         self.max_width = np.array([p["maxd"] for p in prepared], dtype=np.int32)
         sizes = D * self.max_width
         self.tmpl_off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64) if C else np.zeros(0, np.int64)
-        tm = np.empty(int(np.sum(sizes)), dtype=np.float64)
-        for c, p in enumerate(prepared):
-            rows = np.pad(p["tmpl"], ((0, 0), (0, p["maxd"] - p["tmpl"].shape[1])), constant_values=1.0)
-            tm[self.tmpl_off[c]:self.tmpl_off[c] + sizes[c]] = rows.ravel()
         cat = lambda k, dt: np.concatenate([np.asarray(p[k], dtype=dt) for p in prepared])
+        on_device = [p["tmpl"] is None for p in prepared]
+        if any(on_device) and not all(on_device):
+            raise ValueError("a curve set's templates are all built on the host or all on the device")
+        if all(on_device):
+            # every curve's template rows and overshoots built on the GPU in one call
+            planets = {p["planet"] for p in prepared}
+            if len(planets) != 1:
+                raise ValueError("one template planet per curve set")
+            tm_dev = torch.empty(int(np.sum(sizes)), dtype=torch.float64, device=self.dev)
+            ov_dev = torch.empty(int(self.dur_off[-1]), dtype=torch.float64, device=self.dev)
+            _lib.template_cache(planets.pop(), [p["samples"] for p in prepared], self.dur_off, cat("widths", np.int32),
+                                self.tmpl_off, self.max_width, ov_dev, tm_dev, device=device)
+            ov = _d2h(ov_dev)
+            for c, p in enumerate(prepared):
+                p["overshoot"] = ov[self.dur_off[c]:self.dur_off[c + 1]]
+        else:
+            tm = np.empty(int(np.sum(sizes)), dtype=np.float64)
+            for c, p in enumerate(prepared):
+                rows = np.pad(p["tmpl"], ((0, 0), (0, p["maxd"] - p["tmpl"].shape[1])), constant_values=1.0)
+                tm[self.tmpl_off[c]:self.tmpl_off[c] + sizes[c]] = rows.ravel()
+            tm_dev = _h2d(torch, tm, self.dev)
+            ov_dev = _h2d(torch, cat("overshoot", np.float64), self.dev)
         self.curves = dict(t=_h2d(torch, cat("t", np.float64), self.dev),
                            y=_h2d(torch, cat("y", np.float64), self.dev),
                            dy=_h2d(torch, cat("dy", np.float64), self.dev),
                            sample_off=self.sample_off, span=self.span)
-        self.tables = dict(widths=_h2d(torch, cat("widths", np.int32), self.dev),
-                           overshoot=_h2d(torch, cat("overshoot", np.float64), self.dev),
-                           templates=_h2d(torch, tm, self.dev),
+        self.tables = dict(widths=_h2d(torch, cat("widths", np.int32), self.dev), overshoot=ov_dev,
+                           templates=tm_dev,
                            dur_off=self.dur_off, tmpl_off=self.tmpl_off, max_width=self.max_width)
         # every curve's own trial periods (ascending), resident for the main pass
         self.period_off = np.concatenate([[0], np.cumsum([len(p["periods"]) for p in prepared])]).astype(np.int64)
@@ -105,10 +122,27 @@ class CurveSetOnDevice:
                                  pass_, precision, device=self.device, want_loc=want_loc, timing=timing)
 
 
-def prepare_curve(t, y, dy, opts, device=0):
+def template_planet(opts):
+    """(per, rp, a, inc, u1, u2) of the template planet of ``opts`` (the
+    reference's "default", "grazing" or "box" template after validate_args);
+    linear limb darkening has u2 = 0."""
+    u = list(np.atleast_1d(opts.u))
+    if opts.limb_dark == "linear":
+        u = [u[0] if len(u) else 0.0, 0.0]
+    elif opts.limb_dark != "quadratic":
+        raise ValueError("limb_dark must be 'quadratic' or 'linear'")
+    if opts.ecc != 0:
+        raise ValueError("only circular template orbits (ecc=0) are supported")
+    return (float(opts.per), float(opts.rp), float(opts.a), float(opts.inc), float(u[0]), float(u[1]))
+
+
+def prepare_curve(t, y, dy, opts, device=0, templates="host"):
     """Clean one curve and build its grids and templates as ``gtls.power`` does
     (main.py:86-148 of the reference): period grid, duration grid, template
-    cache deduplicated by width."""
+    cache deduplicated by width.  ``templates="device"`` leaves the template
+    rows and overshoots to ``CurveSetOnDevice`` (built on the GPU for all
+    curves at once, ``gtls_template_cache``); the widths and durations, which
+    depend on the grids alone, are set here."""
     t, y, dy = validate_inputs(t, y, dy)
     if len(opts.periods) == 0:
         periods = period_grid(R_star=opts.R_star, M_star=opts.M_star, time_span=np.max(t) - np.min(t),
@@ -121,14 +155,27 @@ def prepare_curve(t, y, dy, opts, device=0):
     maxwidth = int(np.max(durations) * np.size(y))
     if maxwidth % 2 != 0:
         maxwidth = maxwidth + 1
-    overview, lc_arr = template.get_cache(durations=durations, maxwidth_in_samples=maxwidth, per=opts.per,
-                                          rp=opts.rp, a=opts.a, inc=opts.inc, ecc=opts.ecc, w=opts.w, u=opts.u,
-                                          limb_dark=opts.limb_dark, verbose=False)
-    widths, overshoot, durs, tmpl, maxd = template.device_templates(lc_arr, overview)
+    if templates == "device":
+        # get_cache's widths (transit.py:119-121) and device_templates' dedup (core.py:605-614)
+        dur = np.asarray(durations, dtype=np.float64)
+        occupied = np.array([int((d / np.max(dur)) * maxwidth) for d in dur], dtype=np.int64)
+        widths, first = np.unique(occupied, return_index=True)
+        widths = widths.astype(np.int32)
+        durs = dur[first]
+        overshoot, tmpl = None, None
+        maxd = int(np.max(widths)) + int(np.max(widths)) % 2
+        planet = template_planet(opts)
+    else:
+        overview, lc_arr = template.get_cache(durations=durations, maxwidth_in_samples=maxwidth, per=opts.per,
+                                              rp=opts.rp, a=opts.a, inc=opts.inc, ecc=opts.ecc, w=opts.w, u=opts.u,
+                                              limb_dark=opts.limb_dark, verbose=False)
+        widths, overshoot, durs, tmpl, maxd = template.device_templates(lc_arr, overview)
+        planet = None
     return dict(t=np.ascontiguousarray(t, dtype=np.float64), y=np.ascontiguousarray(y, dtype=np.float64),
                 dy=np.ascontiguousarray(dy, dtype=np.float64), periods=np.ascontiguousarray(periods),
                 span=float(np.float32(np.max(t) - np.min(t))), widths=widths, overshoot=overshoot,
-                durations=durs, tmpl=tmpl, maxd=int(maxd), duration_grid=np.asarray(durations))
+                durations=durs, tmpl=tmpl, maxd=int(maxd), duration_grid=np.asarray(durations),
+                samples=int(maxwidth), planet=planet)
 
 
 def _offsets(counts):
@@ -144,7 +191,10 @@ class gtls_batch(object):
     True adds transit times and the SNRs) and ``keep_spectra`` (default
     True: each result carries its periods, power and chi2) and ``autotune``
     (default True: launch shapes timed and chosen on the data, see
-    ``gtls_b200.tune``; results do not depend on them); ``refine=True``
+    ``gtls_b200.tune``; results do not depend on them), ``templates``
+    ("device", default: every curve's template tables built on the GPU in one
+    call, ``gtls_template_cache``; "host": the reference's host construction,
+    ``template.get_cache``; the two agree to about 1e-15); ``refine=True``
     refines every curve's best peak in one batched adjoint run (see
     ``refine_results``).  With
     ``distributed=True`` under an initialised torch.distributed process group
@@ -161,6 +211,9 @@ class gtls_batch(object):
         full_stats = bool(kwargs.pop("full_stats", False))
         autotune = bool(kwargs.pop("autotune", True))
         keep_spectra = bool(kwargs.pop("keep_spectra", True))
+        templates = kwargs.pop("templates", "device")
+        if templates not in ("device", "host"):
+            raise ValueError('templates must be "device" or "host"')
         timing = kwargs.pop("timing", None)
         phases = kwargs.pop("phases", None)
         kwargs.setdefault("precision", "fp32")
@@ -179,7 +232,7 @@ class gtls_batch(object):
                 sub = types.SimpleNamespace(**vars(opts))
                 sub.batch_periods = np.asarray(opts.batch_periods)[list(indices)]
             ph = core.Phases(phases)
-            prepared = [prepare_curve(*self.curves[i], sub, device=device) for i in indices]
+            prepared = [prepare_curve(*self.curves[i], sub, device=device, templates=templates) for i in indices]
             ph.mark("prepare_curves")
             out = search_prepared(prepared, sub, device=device, full_stats=full_stats,
                                   keep_spectra=keep_spectra, timing=timing, autotune=autotune, phases=phases)

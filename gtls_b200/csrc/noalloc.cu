@@ -21,7 +21,10 @@
 //    between calls;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, which also loads the module on that device); make
-//    that first call before any stream capture on the device.
+//    that first call before any stream capture on the device.  The address is
+//    kept for the life of the process, so the entry point must not be used on
+//    a device after a cudaDeviceReset of it (the module, and the array with
+//    it, may then be loaded at another address).
 #include <cuda_runtime.h>
 
 #include <atomic>

@@ -268,6 +268,42 @@ int gtls_spectra(gtls_ctx* ctx, const double* chi2, const uint8_t* mask, int64_t
                  double* sde_raw, double* sde, void* stream);
 
 /*
+ * Transit template tables for many light curves, built on the device the
+ * way the reference builds its template cache on the host
+ * (transit.py:8-160: reference_transit, fractional_transit, get_cache,
+ * through core.py:753-754's 1 - pad(template)).  The template planet (a
+ * circular orbit of period `per` days, radius rp and semi-major axis a in
+ * stellar radii, inclination `inc` degrees, quadratic limb darkening u1, u2;
+ * the reference's "default", "grazing" and "box" templates are parameter
+ * sets of it) is sampled on 10,000 points over one day with the limb-darkened
+ * occultation integral (batman in the reference), trimmed to its in-transit
+ * part, interpolated to each curve's `samples` (its maximum template width)
+ * and rescaled; for every row r of curve c (widths[r], ascending unique
+ * widths in [1, samples[c]]) it is squeezed to widths[r] samples, scaled to
+ * depth 0.5 and trimmed to the samples below 1 - 1e-8.  Outputs (device):
+ * overshoot[r] = 1 / (2 - mean / min) of the trimmed template, and the row
+ * 1 - template padded with 1 to row_len[c] values at
+ * templates[tmpl_off[c] + (r - row_off[c]) * row_len[c]].  Fails with
+ * GTLS_E_INVALID if a row has no sample below 1 - 1e-8.  Synchronises the
+ * stream.
+ */
+typedef struct gtls_template_desc {
+  int32_t abi_version;        /* GTLS_ABI_VERSION                               */
+  int32_t n_curves;
+  double per, rp, a, inc;     /* template planet (days, stellar radii, degrees) */
+  double u1, u2;              /* quadratic limb darkening (linear: u2 = 0)      */
+  const int32_t* samples;     /* host [n_curves]: max template width, >= 2      */
+  const int64_t* row_off;     /* host [n_curves + 1]: rows of curve c           */
+  const int32_t* widths;      /* host [rows]: template width of each row        */
+  const int64_t* tmpl_off;    /* host [n_curves]: offset of curve c's rows      */
+  const int32_t* row_len;     /* host [n_curves]: row length, >= samples[c]     */
+  double* overshoot;          /* device [rows] out                              */
+  double* templates;          /* device out                                     */
+} gtls_template_desc;
+
+int gtls_template_cache(gtls_ctx* ctx, const gtls_template_desc* desc, void* stream);
+
+/*
  * Chi2 of the unfolded limb-darkened transit model and its gradient, for
  * n_curves light curves concatenated in t/y/w (curve c owns samples
  * curve_off[c] .. curve_off[c+1]-1, w = 1/dy^2).  params[6c..6c+5] =
@@ -310,6 +346,9 @@ int gtls_model_chi2_grad(gtls_ctx* ctx, const double* t, const double* y, const 
  *     on the GPU race; each call writes every scratch value it reads;
  *   - the first call on a device looks up the array's address (and loads the
  *     library's device code there): make it before any stream capture;
+ *   - that address is kept for the life of the process: do not call it on a
+ *     device after a cudaDeviceReset of that device (the array may then sit
+ *     at another address);
  *   - synchronises the stream; errors are described by
  *     gtls_noalloc_last_error() (thread-local).
  */

@@ -44,7 +44,8 @@ def test_ctypes_descriptors_match_the_c_layout(tmp_path):
     if cc is None:
         import pytest
         pytest.skip("no C compiler")
-    structs = {"gtls_search_desc": _lib.SearchDesc, "gtls_batch_desc": _lib.BatchDesc, "gtls_timing": _lib.Timing}
+    structs = {"gtls_search_desc": _lib.SearchDesc, "gtls_batch_desc": _lib.BatchDesc, "gtls_timing": _lib.Timing,
+               "gtls_template_desc": _lib.TemplateDesc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gtls_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))

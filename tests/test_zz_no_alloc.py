@@ -34,8 +34,9 @@ def test_noalloc_spectra_matches_allocating_entry_point(cuda):
     from gtls_b200 import _lib
     lib = _lib.load()
     rng = np.random.default_rng(5)
-    # two calls in a row with different inputs (the second reuses the static scratch)
-    for n, osf, nmask in [(20000, 3, 0), (7001, 2, 11)]:
+    # calls in a row with different inputs (each reuses the static scratch);
+    # the last has n <= 2 * kernel (91 here), where no running median is taken
+    for n, osf, nmask in [(20000, 3, 0), (7001, 2, 11), (150, 3, 5)]:
         chi2 = torch.from_numpy(1000 + rng.normal(0, 3, n)).cuda()
         m = np.zeros(n, np.uint8)
         m[rng.choice(n, nmask, replace=False)] = 1
