@@ -721,6 +721,35 @@ def bench_cfg3(args):
         c32, c64 = a.diagnostics["chi2_main"], b.diagnostics["chi2_main"]
         ok = np.isfinite(c64) & np.isfinite(c32)
         spec.append(float(np.max(np.abs(c32[ok] - c64[ok]) / np.abs(c64[ok]))))
+    # against the FP64 oracle (tests/golden/cfg3_oracle.npz, made by
+    # tests/golden/make_cfg3_oracle.py from the reference's kernels built for the CPU)
+    vs_oracle = None
+    fx_path = os.path.join(ROOT, "tests", "golden", "cfg3_oracle.npz")
+    if os.path.exists(fx_path):
+        fx = np.load(fx_path)
+        k = min(int(fx["n_seeds"]), len(curves))
+        forms = {"fp32_per_curve": [(r.diagnostics["period_index"], r.durationPoints, r.SDE, r.depth, r.T0,
+                                     np.ma.getdata(r.chi2)) for r in r32],
+                 "fp64_per_curve": [(r.diagnostics["period_index"], r.durationPoints, r.SDE, r.depth, r.T0,
+                                     np.ma.getdata(r.chi2)) for r in r64],
+                 "batched_fp32": [(r.period_index, r.width, r.SDE, r.depth, r.T0, np.ma.getdata(r.chi2)) for r in rb]}
+        vs_oracle = {"seeds": k, "what": "FP64 oracle (reference kernels built for the CPU, R64) on the same grids"}
+        for name, vals in forms.items():
+            sc = [fx["seed%d_scalars" % s] for s in range(k)]
+            same = [int(v[0]) == int(o[0]) for v, o in zip(vals, sc)]
+            same_w = [int(v[1]) == int(o[2]) for v, o in zip(vals, sc)]
+            spec = []
+            for v, s in zip(vals, range(k)):
+                o = fx["seed%d_chi2" % s].astype(np.float64)
+                ok = np.isfinite(o) & np.isfinite(v[5])
+                spec.append(float(np.max(np.abs(v[5][ok] / o[ok] - 1))) if np.any(ok) else 0.0)
+            vs_oracle[name] = {"best_period_index_agreement": float(np.mean(same)),
+                               "best_duration_agreement": float(np.mean(same_w)),
+                               "SDE_max_rel_err": float(max(rel(v[2], o[3]) for v, o in zip(vals, sc))),
+                               "depth_max_rel_err": float(max(rel(v[3], o[4]) for v, o in zip(vals, sc))),
+                               "T0_max_abs_err_days": float(max(abs(v[4] - o[5]) for v, o in zip(vals, sc))),
+                               "chi2_spectrum_max_rel_err": float(max(spec)),
+                               "note": "chi2 spectrum against the oracle's stored in float32 (6e-8)"}
     acc = {
         "curves": len(curves),
         "best_period_index_agreement": float(np.mean(same_p)),
@@ -745,7 +774,8 @@ def bench_cfg3(args):
                     "d2h_bytes_per_step": None, "ms_per_step": ms["fp32"]},
             "fp64_per_curve": {"value": 64 * 1000.0 / ms["fp64"], "ms": ms["fp64"]},
             "batched_fp32": {"value": 64 * 1000.0 / ms["batched_fp32"], "ms": ms["batched_fp32"]},
-            "gpu_launches": int(launches), "accuracy": acc, "clocks": clk.summary()}
+            "gpu_launches": int(launches), "accuracy": acc, "accuracy_vs_fp64_oracle": vs_oracle,
+            "clocks": clk.summary()}
     print(json.dumps(line))
     return 0
 

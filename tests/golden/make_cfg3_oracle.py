@@ -2,7 +2,7 @@
 the 64 seeds of the mixed-precision workload (19,728 samples at 2-min
 cadence over 27.4 d, depth log-U(100, 2000) ppm, P log-U(1, 500) d): for each
 seed the best period index and period, the width, SDE, depth, T0 and
-duration, and the chi2 spectrum, from the oracle's host flow
+duration, and the chi2 spectrum (stored in float32), from the oracle's host flow
 (oracle/tls_oracle.search, core.py:568-999) over the reference's kernels
 compiled for the CPU in FP64 (oracle/_ref, R64).  Grid, templates and
 duration-union batch size are the ones gtls().power() uses on a GPU whose
@@ -47,7 +47,7 @@ def main(n_seeds):
         r = O.search(be, P, t, y, dy, widths, tm, os_, dd, maxd, 1e-5, 0.125, 3, batch=batch)
         out["seed%d_scalars" % seed] = np.array([r["period_index"], r["period"], r["width"], r["SDE"], r["depth"],
                                                  r["T0"], r["duration"], batch], dtype=np.float64)
-        out["seed%d_chi2" % seed] = np.ma.getdata(r["chi2"]).astype(np.float64)
+        out["seed%d_chi2" % seed] = np.ma.getdata(r["chi2"]).astype(np.float32)   # ample for 2e-6 bars
         print("seed", seed, r["period_index"], r["SDE"], flush=True)
         np.savez_compressed(os.path.join(HERE, "cfg3_oracle.npz"), n_seeds=np.array(seed + 1), **out)
 

@@ -334,3 +334,19 @@ def test_best_period_statistics_match_reference():
         np.testing.assert_array_equal(mask, g["mask"])
         pink = [stats.pink_noise(y[~mask], w) for w in (1, 5, 37)]
         np.testing.assert_allclose(pink, g["pink"], rtol=1e-12, atol=1e-300)
+
+
+def test_cfg3_oracle_fixture_matches_the_product_grid():
+    """The FP64-oracle fixture of the mixed-precision workload (64 seeds)
+    was made on the grids power() uses: same period count, and the recorded
+    best period is the grid point at the recorded index."""
+    from gtls_b200 import synthetic, validate as V
+    f = golden("cfg3_oracle")
+    assert int(f["n_seeds"]) == 64
+    for seed in (0, 31, 63):
+        t, y, dy, _ = synthetic.light_curve_cfg3(seed)
+        t, y, dy = V.validate_inputs(t, y, dy)
+        P = G.period_grid(1, 1, t.max() - t.min(), 0.5, 13.7, 3, 2, ascending=True)
+        sc = f["seed%d_scalars" % seed]
+        assert len(f["seed%d_chi2" % seed]) == len(P)
+        assert P[int(sc[0])] == sc[1]
