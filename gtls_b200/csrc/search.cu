@@ -53,7 +53,12 @@ namespace gtls {
 
 constexpr int kPrepThreads = 1024;
 constexpr int kSmallBucket = 8;     // entries of buckets up to this size are ranked by their own thread
+constexpr int kSmallBucketSm = 16;  // the same, for buckets in shared memory
 constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (warp-ranked)
+constexpr int kMaxRounds = 32;      // rounds of the shared-memory prepare path
+constexpr int kRoundShift = 20;     // hist entries of that path: position | round << kRoundShift
+constexpr int kPosMask = (1 << kRoundShift) - 1;
+constexpr int kPrepStaticSmem = 4096;  // static shared memory of prepare_kernel, rounded up
 constexpr int kChiThreads = 512;
 constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset rho
 // Split-path task: a window of kWin consecutive starts of one duration.  Its
@@ -129,6 +134,7 @@ struct CurveDev {
   long long np;
   int n, maxd, M, Mrec, D, max_width, batch, nbatch;
   int tile, ntiles, nb_log2;
+  int rnb_log2, rcap;           // shared-memory prepare path: bucket bits and round capacity (0: off)
   int global_rec;               // 1: chi2 reads the records from global memory (no shared tile)
   float span;
 };
@@ -234,13 +240,12 @@ __device__ __forceinline__ double fold_phase(double t, double P) {
   return x - (double)(int)x;
 }
 
-// Bucket of a phase: floor(phase * NB) (exact: NB is a power of two),
-// clamped so that out-of-range phases land in the first or last bucket.
-__device__ __forceinline__ int phase_bin(double ph, int nb_log2) {
-  double x = ldexp(ph, nb_log2);
+// Bucket of a phase from x = phase * NB (exact: NB = scale is a power of
+// two, and |phase| < 1): floor(x), clamped so that out-of-range phases land
+// in the first or last bucket.
+__device__ __forceinline__ int phase_bin(double x, int nb) {
   int b = (int)x;
   b = b < 0 ? 0 : b;
-  int nb = 1 << nb_log2;
   return b >= nb ? nb - 1 : b;
 }
 
@@ -288,6 +293,359 @@ __device__ __forceinline__ void rank_bucket_warp(const uint2* __restrict__ slot,
   }
 }
 
+// Prefix of v in place over pre[1..M], accumulated in FP64 for both forms
+// (the FP32 form then stores each prefix as a float-float pair (hi, lo) in
+// the same 8 bytes): each warp scans a contiguous range (coalesced), then
+// adds the sum of the ranges before it.  pre[0] = 0.  wsum: 32 doubles.
+template <typename Real>
+__device__ void prefix_of_v(double* pre_d, int M, double* wsum) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int per = (M + nwarp - 1) / nwarp;
+  const int beg = 1 + min(M, wid * per);
+  const int end = 1 + min(M, (wid + 1) * per);
+  double acc = 0.0;
+  for (int r = beg + lane; r < end; r += 32) acc += pre_d[r];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) wsum[wid] = acc;
+  __syncthreads();
+  double carry = 0.0;
+  for (int w = 0; w < wid; ++w) carry += wsum[w];
+  if (wid == 0 && lane == 0) store_prefix<Real>(pre_d, 0, 0.0);
+  for (int r0 = beg; r0 < end; r0 += 32) {
+    const int r = r0 + lane;
+    double x = r < end ? pre_d[r] : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double yv = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += yv;
+    }
+    if (r < end) store_prefix<Real>(pre_d, r, carry + x);
+    carry += __shfl_sync(0xffffffffu, x, 31);
+  }
+}
+
+// Prefix value at pre[r] as a double (the inverse of store_prefix; in the
+// FP32 form the float-float pair is summed back in FP64).
+template <typename Real>
+__device__ __forceinline__ double load_prefix(const double* pre, int r) {
+  if constexpr (sizeof(Real) == 8) {
+    return pre[r];
+  } else {
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(pre[r]);
+    return (double)__uint_as_float((unsigned)bits) + (double)__uint_as_float((unsigned)(bits >> 32));
+  }
+}
+
+// Inclusive prefix of src[0, cnt) (shared memory, FP64) plus carry0, stored
+// at pre[dst0 + q] for q < cnt; returns, in every thread, the last stored
+// value (carry0 when cnt == 0).  Thread i sums its own chunk of K
+// consecutive entries (K odd, so that the lanes' strided reads fall in
+// distinct banks), the chunk sums are scanned across the block (shuffles,
+// then the warp totals), each thread rewrites its chunk in place as the
+// running prefix, and the block stores the result coalesced.  wsum: 32
+// doubles.  Ends with a barrier, after which src may be overwritten.
+template <typename Real>
+__device__ double scan_store(double* src, int cnt, double carry0, double* pre_d, int dst0, double* wsum) {
+  if (cnt <= 0) return carry0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int K = ((cnt + blockDim.x - 1) / blockDim.x) | 1;
+  const int beg = min(cnt, (int)threadIdx.x * K), end = min(cnt, beg + K);
+  double acc = 0.0;
+  for (int r = beg; r < end; ++r) acc += src[r];
+  // exclusive prefix of the chunk sums: within the warp, then over the warps
+  double inc = acc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double yv = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += yv;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  double exc = __shfl_up_sync(0xffffffffu, inc, 1);
+  double run = carry0;
+  for (int w = 0; w < wid; ++w) run += wsum[w];
+  if (lane > 0) run += exc;
+  for (int r = beg; r < end; ++r) {
+    run += src[r];
+    src[r] = run;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < cnt; q += blockDim.x) store_prefix<Real>(pre_d, dst0 + q, src[q]);
+  const double last = src[cnt - 1];
+  __syncthreads();
+  return last;
+}
+
+// Round tables of the shared-memory prepare path.
+struct RoundTables {
+  int nrounds;               // rounds; -1: the period takes the global-scatter path
+  int rb[kMaxRounds + 1];    // first bucket of each round (rb[nrounds] = NB)
+  int rpos[kMaxRounds + 1];  // first sorted position of each round (rpos[nrounds] = n)
+  int cursor[kMaxRounds];    // append cursors of the round-partitioned sample words
+};
+
+// Shared-memory prepare of one period (curves of at most kPackedMaxN
+// samples).  The samples are folded (GPUFun.py:30-41) and counted into NB
+// phase buckets; the buckets are cut greedily into rounds of whole buckets
+// holding at most `cap` samples each; a second fold appends each sample's
+// word (in-bucket key, index | bucket << kPackedShift) to its round's range
+// of the scratch row `stage` (warp-aggregated, so the stores stay nearly
+// coalesced).  Each round then
+//   (a) reads its words (coalesced) into shared-memory slots by bucket,
+//   (b) ranks every slot within its bucket (the stable argsort order of
+//       the fold, as slot_less defines it) and writes the record of the
+//       resulting sorted position (close to the slot's, so nearly
+//       coalesced), with its v into shared memory, and
+//   (c) stores the FP64 prefix of v over its positions,
+// so that nothing is scattered through global memory.  Afterwards the
+// wrapped copy of the first maxd positions (patchData, GPUFun.py:110-129)
+// gets its prefix from pre[n] + pre[q + 1].  Returns false, having written
+// nothing, when a single bucket holds more than `cap` samples or more than
+// kMaxRounds rounds would be needed; the caller then takes the global path.
+// Dynamic shared memory: hist [NB] ints, slots [cap] words, vbuf [cap]
+// doubles.
+template <typename Real, bool kOrder>
+__device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum, int* big, int* nbig, RoundTables& rt,
+                               const double* __restrict__ t, const double2* __restrict__ vw, int n, int maxd,
+                               double P, int nb_log2, int cap, uint2* __restrict__ stage,
+                               typename Tr<Real>::R2* __restrict__ out, double* __restrict__ pre_d,
+                               int* __restrict__ ord) {
+  using R2 = typename Tr<Real>::R2;
+  const int nb = 1 << nb_log2;
+  const double scale = (double)nb;
+  constexpr unsigned imask = (unsigned)(kPackedMaxN - 1);
+  int* hist = dyn;
+  uint2* slots = reinterpret_cast<uint2*>(dyn + nb);
+  double* vbuf = reinterpret_cast<double*>(slots + cap);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  constexpr int kB = 4;   // elements per thread in flight in each pass
+  const int stride = blockDim.x * kB;
+
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  // (1) fold and histogram of buckets
+  for (int i0 = threadIdx.x; i0 < n; i0 += stride) {
+    double tv[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      tv[u] = i < n ? t[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) atomicAdd(&hist[phase_bin(fold_phase(tv[u], P) * scale, nb)], 1);
+    }
+  }
+  __syncthreads();
+  block_exclusive_scan_smem(hist, nb, wtmp_i);   // hist[b]: first position of bucket b
+  // (2) rounds, by warp 0: from bucket b0, the largest b1 with
+  //     start(b1) <= start(b0) + cap (a 32-way search of the bucket starts)
+  if (wid == 0) {
+    auto S = [&](int x) { return x < nb ? hist[x] : n; };
+    int r = 0, b0 = 0;
+    bool ok = true;
+    if (lane == 0) {
+      rt.rb[0] = 0;
+      rt.rpos[0] = 0;
+    }
+    while (b0 < nb) {
+      const int lim = S(b0) + cap;
+      int lo = b0, hi = nb;   // S(lo) <= lim; the answer lies in [lo, hi]
+      while (lo < hi) {
+        const int step = (hi - lo + 31) >> 5;
+        const int x = min(hi, lo + (lane + 1) * step);
+        const int c = __popc(__ballot_sync(0xffffffffu, S(x) <= lim));   // a prefix of the lanes
+        const int nlo = min(hi, lo + c * step);
+        const int nhi = c == 32 ? hi : min(hi, lo + (c + 1) * step) - 1;
+        lo = nlo;
+        hi = nhi;
+      }
+      if (lo == b0 || r == kMaxRounds) {   // bucket b0 alone exceeds cap, or too many rounds
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        rt.cursor[r] = S(b0);
+        rt.rb[r + 1] = lo;
+        rt.rpos[r + 1] = S(lo);
+      }
+      ++r;
+      b0 = lo;
+    }
+    if (lane == 0) rt.nrounds = ok ? r : -1;
+  }
+  __syncthreads();
+  const int nr = rt.nrounds;
+  if (nr < 0) return false;
+  // each bucket's round in the bits of hist above the positions
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    hist[b] |= upper_find(0, nr, b, [&](int q) { return (long long)rt.rb[q]; }) << kRoundShift;
+  auto H = [&](int b) { return hist[b] & kPosMask; };
+  __syncthreads();
+  // (3) fold again; each sample's word to its round's range of the scratch
+  //     row (the loop runs over whole warps for the warp-wide match)
+  for (int i0 = threadIdx.x - lane; i0 < n; i0 += stride) {
+    double tv[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + lane + u * blockDim.x;
+      tv[u] = i < n ? t[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + lane + u * blockDim.x;
+      int r = -1;
+      uint2 wd = make_uint2(0u, 0u);
+      if (i < n) {
+        const double x = fold_phase(tv[u], P) * scale;
+        const int b = phase_bin(x, nb);
+        wd = make_uint2(__float_as_uint((float)(x - (double)b)), (unsigned)i | ((unsigned)b << kPackedShift));
+        r = hist[b] >> kRoundShift;
+      }
+      const unsigned peers = __match_any_sync(0xffffffffu, r);
+      const int leader = __ffs(peers) - 1;
+      int pos = 0;
+      if (lane == leader && r >= 0) pos = atomicAdd(&rt.cursor[r], __popc(peers));
+      pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & ((1u << lane) - 1u));
+      if (r >= 0 && pos < rt.rpos[r + 1]) stage[pos] = wd;   // always true: the counts of pass (1)
+    }
+  }
+  __syncthreads();
+  double carry = 0.0;   // prefix of v up to the current round (FP64)
+  for (int r = 0; r < nr; ++r) {
+    const int rs = rt.rpos[r], cnt = rt.rpos[r + 1] - rs;
+    const int b0 = rt.rb[r], b1 = rt.rb[r + 1];
+    // (a) the round's words into slots by bucket; afterwards the position
+    //     H(b) is the end of bucket b and H(b - 1) its start (for the round's
+    //     first bucket that is the end of the previous round's last one, rs)
+    for (int q0 = threadIdx.x; q0 < cnt; q0 += stride) {
+      uint2 wd[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int q = q0 + u * blockDim.x;
+        wd[u] = q < cnt ? stage[rs + q] : make_uint2(0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int q = q0 + u * blockDim.x;
+        if (q < cnt) {
+          const int b = (int)(wd[u].y >> kPackedShift);
+          const int sl = (atomicAdd(&hist[b], 1) & kPosMask) - rs;
+          if ((unsigned)sl < (unsigned)cnt) slots[sl] = wd[u];   // always true: the counts of pass (1)
+        }
+      }
+    }
+    if (threadIdx.x == 0) *nbig = 0;
+    __syncthreads();
+    // (b) ranks, and the records at once: the entry of sorted position p
+    //     (round-local q = p - rs) and original sample i gets its record
+    //     (u, w) at p (and at p + n when p < maxd: the wrap of patchData,
+    //     GPUFun.py:110-129) and its v at vbuf[q]; i is clamped so that a
+    //     malformed input can never address outside the curve.  Buckets of
+    //     more than kSmallBucketSm entries are listed and ranked by whole warps
+    //     (unless the list overflows); every other slot by its own thread.
+    for (int b = b0 + (int)threadIdx.x; b < b1; b += blockDim.x) {
+      const int k = H(b) - (b == 0 ? 0 : H(b - 1));
+      if (k > kSmallBucketSm) {
+        const int q = atomicAdd(nbig, 1);
+        if (q < kBigBuckets) big[q] = b;
+      }
+    }
+    __syncthreads();
+    const int nbg = *nbig;
+    const bool warp_ranked = nbg <= kBigBuckets;
+    auto emit = [&](int q, int i) {
+      i = min(max(i, 0), n - 1);
+      const int p = rs + q;
+      if constexpr (kOrder) {
+        ord[p] = i;
+        return;
+      }
+      const double2 g = vw[i];
+      R2 o;
+      o.x = (Real)(g.x * g.y);
+      o.y = (Real)g.y;
+      out[p] = o;
+      if (p < maxd) out[p + n] = o;
+      vbuf[q] = g.x;
+    };
+    if (warp_ranked)
+      for (int q = wid; q < nbg; q += nwarp) {
+        const int b = big[q];
+        rank_bucket_warp(slots, (b == 0 ? 0 : H(b - 1)) - rs, H(b) - rs, t, P, imask, emit);
+      }
+    for (int j0 = threadIdx.x; j0 < cnt; j0 += stride) {
+      int pos[kB], idx[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int j = j0 + u * blockDim.x;
+        pos[u] = -1;
+        idx[u] = 0;
+        if (j < cnt) {
+          const uint2 sj = slots[j];
+          const int b = (int)(sj.y >> kPackedShift);
+          const int s = (b == 0 ? 0 : H(b - 1)) - rs;
+          const int e = H(b) - rs;
+          idx[u] = (int)(sj.y & imask);
+          if (e - s == 1) {
+            pos[u] = j;
+          } else if (e - s <= kSmallBucketSm || !warp_ranked) {
+            // entries of smaller key, and of equal key (itself included);
+            // equal keys, rare, are then ordered on the exact phases
+            const float kj = __uint_as_float(sj.x);
+            int lt = 0, eq = 0;
+#pragma unroll 4
+            for (int m = s; m < e; ++m) {
+              const float km = __uint_as_float(slots[m].x);
+              lt += km < kj;
+              eq += km == kj;
+            }
+            if (eq > 1)
+              for (int m = s; m < e; ++m)
+                if (m != j && __uint_as_float(slots[m].x) == kj) lt += slot_less(slots[m], sj, t, P, imask);
+            pos[u] = s + lt;
+          }
+        }
+      }
+      // the gathers of the kB entries in flight together
+      if constexpr (kOrder) {
+#pragma unroll
+        for (int u = 0; u < kB; ++u)
+          if (pos[u] >= 0) emit(pos[u], idx[u]);
+      } else {
+        double2 g[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) g[u] = pos[u] >= 0 ? vw[min(max(idx[u], 0), n - 1)] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          if (pos[u] >= 0) {
+            const int p = rs + pos[u];
+            R2 o;
+            o.x = (Real)(g[u].x * g[u].y);
+            o.y = (Real)g[u].y;
+            out[p] = o;
+            if (p < maxd) out[p + n] = o;
+            vbuf[pos[u]] = g[u].x;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // (c) pre[rs + q + 1] = carry + v[0..q] (ends with a barrier)
+    if constexpr (!kOrder) carry = scan_store<Real>(vbuf, cnt, carry, pre_d, rs + 1, wsum);
+  }
+  if constexpr (!kOrder) {
+    // pre[0] = 0, and the wrapped copy: pre[n + 1 + q] = pre[n] + pre[q + 1]
+    if (threadIdx.x == 0) store_prefix<Real>(pre_d, 0, 0.0);
+    const int nw = min(maxd, n);
+    for (int q = threadIdx.x; q < nw; q += blockDim.x)
+      store_prefix<Real>(pre_d, n + 1 + q, carry + load_prefix<Real>(pre_d, q + 1));
+  }
+  return true;
+}
+
 // kOrder: write only the stable fold order of each period (order_out[rec_off
 // + local * n + p] = original index of sorted position p) instead of the
 // records and prefix (gtls_fold_order).
@@ -314,6 +672,7 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   const int maxd = C.maxd;
   const int nb_log2 = C.nb_log2;
   const int nb = 1 << nb_log2;
+  const double scale = (double)nb;
   const bool packed = n <= kPackedMaxN && nb_log2 <= 32 - kPackedShift;
   const unsigned imask = packed ? (unsigned)(kPackedMaxN - 1) : 0xffffffffu;
   const double P = C.periods[R.pidx0 + local];
@@ -326,6 +685,11 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   int* ord = kOrder ? order_out + R.rec_off + (size_t)local * n : nullptr;
   constexpr int kB = 4;   // elements per thread in flight in each pass
   const int stride = blockDim.x * kB;
+  __shared__ RoundTables rt;
+  if (C.rnb_log2 > 0 && prepare_rounds<Real, kOrder>(hist, wtmp_i, wsum, big, &nbig, rt, t, vw, n, maxd, P,
+                                                     C.rnb_log2, C.rcap, slot, out, pre_d, ord))
+    return;
+  // global path: buckets scattered through the scratch row
 
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
   if (threadIdx.x == 0) nbig = 0;
@@ -341,7 +705,7 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
       const int i = i0 + u * blockDim.x;
-      if (i < n) atomicAdd(&hist[phase_bin(fold_phase(tv[u], P), nb_log2)], 1);
+      if (i < n) atomicAdd(&hist[phase_bin(fold_phase(tv[u], P) * scale, nb)], 1);
     }
   }
   __syncthreads();
@@ -359,10 +723,10 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
     for (int u = 0; u < kB; ++u) {
       const int i = i0 + u * blockDim.x;
       if (i < n) {
-        const double ph = fold_phase(tv[u], P);
-        const int b = phase_bin(ph, nb_log2);
+        const double x = fold_phase(tv[u], P) * scale;
+        const int b = phase_bin(x, nb);
         const int s = atomicAdd(&hist[b], 1);
-        const float f = (float)(ldexp(ph, nb_log2) - (double)b);
+        const float f = (float)(x - (double)b);
         slot[s] = make_uint2(__float_as_uint(f), (unsigned)i | (packed ? (unsigned)b << kPackedShift : 0u));
       }
     }
@@ -446,34 +810,9 @@ prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ r
   }
   __syncthreads();
   if constexpr (kOrder) return;
-  // (5) prefix of v in place over pre[1..M], accumulated in FP64 for both
-  //     forms (the FP32 form then stores each prefix as a float-float pair
-  //     (hi, lo) in the same 8 bytes): each warp scans a contiguous range
-  //     (coalesced), then adds the sum of the ranges before it
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int per = (M + nwarp - 1) / nwarp;
-  const int beg = 1 + min(M, wid * per);
-  const int end = 1 + min(M, (wid + 1) * per);
-  double acc = 0.0;
-  for (int r = beg + lane; r < end; r += 32) acc += pre_d[r];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) wsum[wid] = acc;
-  __syncthreads();
-  double carry = 0.0;
-  for (int w = 0; w < wid; ++w) carry += wsum[w];
-  if (wid == 0 && lane == 0) store_prefix<Real>(pre_d, 0, 0.0);
-  for (int r0 = beg; r0 < end; r0 += 32) {
-    const int r = r0 + lane;
-    double x = r < end ? pre_d[r] : 0.0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const double yv = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += yv;
-    }
-    if (r < end) store_prefix<Real>(pre_d, r, carry + x);
-    carry += __shfl_sync(0xffffffffu, x, 31);
-  }
+  // (5) prefix of v in place over pre[1..M] (accumulated in FP64; the FP32
+  //     form stores float-float pairs)
+  prefix_of_v<Real>(pre_d, M, wsum);
 }
 
 // ------------------------------------------------------------------ chi2
@@ -1151,6 +1490,35 @@ static int nb_log2_for(int n, int shift) {
   return std::max(1, k);
 }
 
+// Shared-memory prepare path of a curve of n samples: NB = 2^(ceil(log2 n) -
+// 2 + shift) buckets (at most 2^14, about four samples a bucket), and the
+// largest round capacity that fits the CTA's shared memory next to them
+// (16 bytes a sample: slot word and v).  Off (0) for curves beyond
+// the packed slot words or when fewer than 1,024 samples fit a round.
+template <typename Real>
+static void rounds_params(CurveDev<Real>& C, int smem_optin, int shift) {
+  C.rnb_log2 = 0;
+  C.rcap = 0;
+  const int n = C.n;
+  if (n < 1 || n > kPackedMaxN) return;
+  int k = 1;
+  while ((1 << k) < n) ++k;
+  const int nbl = std::max(1, std::min(14, k - 2 + shift));
+  const long long c = std::min<long long>(((long long)smem_optin - kPrepStaticSmem - (4LL << nbl)) / 16, n);
+  if (c < 1024 && c < n) return;
+  C.rnb_log2 = nbl;
+  C.rcap = (int)c;
+}
+// Dynamic shared memory of prepare_kernel for a curve: the larger of the
+// two paths' needs (a period falls back to the global path when its
+// buckets do not fit the rounds).
+template <typename Real>
+static size_t prep_smem_bytes(const CurveDev<Real>& C) {
+  size_t b = sizeof(int) << C.nb_log2;
+  if (C.rnb_log2 > 0) b = std::max(b, (sizeof(int) << C.rnb_log2) + 16 * (size_t)C.rcap);
+  return b;
+}
+
 // One light curve of a search, as the host sees it.
 struct CurveHost {
   const double *t, *y, *dy, *periods;
@@ -1236,6 +1604,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     C.tile = (int)tile;
     C.ntiles = (int)((n + tile - 1) / tile);
     C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
+    rounds_params(C, ctx->smem_optin, ctx->bucket_shift);
     C.global_rec = global_rec ? 1 : 0;
     C.span = h.span;
     p_off[c + 1] = p_off[c] + h.np;
@@ -1339,7 +1708,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
         bytes += (size_t)take * per;
         items += (int)take;
         tiles += (int)(take * C.ntiles);
-        sm_prep = std::max(sm_prep, sizeof(int) << C.nb_log2);
+        sm_prep = std::max(sm_prep, prep_smem_bytes(C));
         sm_chi = std::max(sm_chi, C.global_rec ? (size_t)C.D * (sizeof(Real) + 2 * sizeof(int))
                                                : chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
         mode = C.global_rec;
@@ -1652,6 +2021,7 @@ extern "C" int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const 
   C.M = n;
   C.Mrec = (n + 1) & ~1;
   C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
+  rounds_params(C, ctx->smem_optin, ctx->bucket_shift);
   // chunks of periods sized to the scratch budget (8 bytes of slots per sample and period)
   const long long per_chunk = std::max<long long>(
       1, std::min<long long>((long long)(ctx->chunk_budget / (8 * (size_t)n)), (long long)INT32_MAX));
@@ -1676,7 +2046,7 @@ extern "C" int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const 
   uint2* slots = cv.take<uint2>((size_t)std::min<long long>(per_chunk, n_periods) * n);
   GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_cd, &C, sizeof(C), cudaMemcpyHostToDevice, st));
   GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_runs, runs.data(), sizeof(Run) * runs.size(), cudaMemcpyHostToDevice, st));
-  const size_t smem = sizeof(int) << C.nb_log2;
+  const size_t smem = prep_smem_bytes(C);
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
   for (size_t k = 0; k < runs.size(); ++k) {
