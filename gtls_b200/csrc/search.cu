@@ -1491,19 +1491,21 @@ static int nb_log2_for(int n, int shift) {
 }
 
 // Shared-memory prepare path of a curve of n samples: NB = 2^(ceil(log2 n) -
-// 2 + shift) buckets (at most 2^14, about four samples a bucket), and the
-// largest round capacity that fits the CTA's shared memory next to them
-// (16 bytes a sample: slot word and v).  Off (0) for curves beyond
-// the packed slot words or when fewer than 1,024 samples fit a round.
+// 2) buckets (at most 2^14, about four samples a bucket), and the largest
+// round capacity that fits the CTA's shared memory next to them (16 bytes a
+// sample: slot word and v).  Off (0) for curves beyond the packed slot
+// words or when fewer than 1,024 samples fit a round.  The rounds fix the
+// summation order of the prefix, so they depend on n and the device alone
+// (not on the tuning, which must not change a result).
 template <typename Real>
-static void rounds_params(CurveDev<Real>& C, int smem_optin, int shift) {
+static void rounds_params(CurveDev<Real>& C, int smem_optin) {
   C.rnb_log2 = 0;
   C.rcap = 0;
   const int n = C.n;
   if (n < 1 || n > kPackedMaxN) return;
   int k = 1;
   while ((1 << k) < n) ++k;
-  const int nbl = std::max(1, std::min(14, k - 2 + shift));
+  const int nbl = std::max(1, std::min(14, k - 2));
   const long long c = std::min<long long>(((long long)smem_optin - kPrepStaticSmem - (4LL << nbl)) / 16, n);
   if (c < 1024 && c < n) return;
   C.rnb_log2 = nbl;
@@ -1604,7 +1606,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     C.tile = (int)tile;
     C.ntiles = (int)((n + tile - 1) / tile);
     C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
-    rounds_params(C, ctx->smem_optin, ctx->bucket_shift);
+    rounds_params(C, ctx->smem_optin);
     C.global_rec = global_rec ? 1 : 0;
     C.span = h.span;
     p_off[c + 1] = p_off[c] + h.np;
@@ -2021,7 +2023,7 @@ extern "C" int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const 
   C.M = n;
   C.Mrec = (n + 1) & ~1;
   C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
-  rounds_params(C, ctx->smem_optin, ctx->bucket_shift);
+  rounds_params(C, ctx->smem_optin);
   // chunks of periods sized to the scratch budget (8 bytes of slots per sample and period)
   const long long per_chunk = std::max<long long>(
       1, std::min<long long>((long long)(ctx->chunk_budget / (8 * (size_t)n)), (long long)INT32_MAX));

@@ -91,7 +91,9 @@ typedef struct gtls_tuning {
   int32_t tile_cap_fp32;      /* max starts per chi2 tile (CTA), FP32 form: a multiple of 256 in
                                  [256, 65536], or 0 = 16384.  The shared-memory size caps it too. */
   int32_t tile_cap_fp64;      /* the same for the FP64 form, 0 = 8192                        */
-  int32_t bucket_shift;       /* phase buckets of the fold ordering = 2^min(15, ceil(log2 N) + shift),
+  int32_t bucket_shift;       /* phase buckets of the global-scatter fold ordering (curves above
+                                 2^17 samples, and periods whose phases cluster beyond what the
+                                 shared-memory ordering holds) = 2^min(15, ceil(log2 N) + shift),
                                  shift in [-3, 0] (0 = default)                               */
   int32_t records_global;     /* 1: the chi2 kernel reads the folded records from global memory
                                  (L1/L2) for every curve; 0: from a shared-memory tile when the
