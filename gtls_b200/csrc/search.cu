@@ -94,15 +94,16 @@ __device__ __forceinline__ float2 ff_from_double(double v) {
 }
 // Store prefix value v at pre[r] through the FP64 view of the prefix array:
 // as a double (FP64 form) or as the float-float pair (hi, lo) occupying the
-// same 8 bytes (FP32 form; hi at the lower address).
+// same 8 bytes (FP32 form; hi at the lower address).  Streaming stores: the
+// chi2 kernel reads them back only after the whole chunk is prepared.
 template <typename Real>
 __device__ __forceinline__ void store_prefix(double* pre, int r, double v) {
   if constexpr (sizeof(Real) == 8) {
-    pre[r] = v;
+    __stcs(pre + r, v);
   } else {
     const float2 f = ff_from_double(v);
     const unsigned long long bits = ((unsigned long long)__float_as_uint(f.y) << 32) | __float_as_uint(f.x);
-    pre[r] = __longlong_as_double((long long)bits);
+    __stcs(pre + r, __longlong_as_double((long long)bits));
   }
 }
 
@@ -539,6 +540,15 @@ __device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum,
     }
     if (threadIdx.x == 0) *nbig = 0;
     __syncthreads();
+    // the scratch lines read so far, whole 128-byte lines inside this
+    // period's row, are dropped from L2 without being written back
+    {
+      const uintptr_t row0 = ((uintptr_t)stage + 127) & ~(uintptr_t)127;
+      const uintptr_t lo = max(row0, (uintptr_t)(stage + rs) & ~(uintptr_t)127);
+      const uintptr_t hi = (uintptr_t)(stage + rs + cnt) & ~(uintptr_t)127;
+      for (uintptr_t a = lo + (uintptr_t)threadIdx.x * 128; a < hi; a += (uintptr_t)blockDim.x * 128)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+    }
     // (b) ranks, and the records at once: the entry of sorted position p
     //     (round-local q = p - rs) and original sample i gets its record
     //     (u, w) at p (and at p + n when p < maxd: the wrap of patchData,
@@ -567,8 +577,8 @@ __device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum,
       R2 o;
       o.x = (Real)(g.x * g.y);
       o.y = (Real)g.y;
-      out[p] = o;
-      if (p < maxd) out[p + n] = o;
+      __stcs(out + p, o);
+      if (p < maxd) __stcs(out + p + n, o);
       vbuf[q] = g.x;
     };
     if (warp_ranked)
@@ -625,8 +635,8 @@ __device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum,
             R2 o;
             o.x = (Real)(g[u].x * g[u].y);
             o.y = (Real)g[u].y;
-            out[p] = o;
-            if (p < maxd) out[p + n] = o;
+            __stcs(out + p, o);
+            if (p < maxd) __stcs(out + p + n, o);
             vbuf[pos[u]] = g[u].x;
           }
         }
