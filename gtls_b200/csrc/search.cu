@@ -962,6 +962,46 @@ __device__ __forceinline__ Real warp_reduce_scatter18(const typename Tr<Real>::R
   return v[0];
 }
 
+// correlate() with the template entries of the offset rho taken from the
+// lanes instead of memory: lane q (q < Q) holds T[q*s + rho] in tl, and step
+// q reads it by shuffle.  The products and their order are those of
+// correlate(); only where the template value comes from differs.  All 32
+// lanes must call it (lanes without starts read clamped records and discard
+// the sums).
+template <typename Real, bool kTwoLevel>
+__device__ __forceinline__ void correlate_bc(const typename Tr<Real>::R2* __restrict__ tile, int L, int base, int s,
+                                             typename Tr<Real>::R2 tl, int Q, typename Tr<Real>::R2 (&acc)[kR]) {
+  using R2 = typename Tr<Real>::R2;
+  R2 xs[kR];
+  const int last = L - 1;
+#pragma unroll
+  for (int i = 0; i < kR - 1; ++i) xs[i] = tile[min(base + i * s, last)];
+  R2 pr[kR];
+#pragma unroll
+  for (int r = 0; r < kR; ++r) pr[r] = kTwoLevel ? zero_pair<R2>() : acc[r];
+  int pos = base + (kR - 1) * s;
+  for (int q0 = 0; q0 < Q; q0 += kR) {
+#pragma unroll
+    for (int qq = 0; qq < kR; ++qq) {
+      if (q0 + qq >= Q) break;
+      xs[(qq + kR - 1) % kR] = tile[min(pos, last)];
+      R2 tq;
+      tq.x = __shfl_sync(0xffffffffu, tl.x, q0 + qq);
+      tq.y = __shfl_sync(0xffffffffu, tl.y, q0 + qq);
+      pos += s;
+#pragma unroll
+      for (int r = 0; r < kR; ++r) fma_pair(tq, xs[(qq + r) % kR], pr[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    if (kTwoLevel)
+      add_pair(acc[r], pr[r]);
+    else
+      acc[r] = pr[r];
+  }
+}
+
 // Dynamic shared memory of one chi2 CTA: the record tile (rounded up to 16
 // bytes) followed by the per-duration table (overshoot, width | skip << 16,
 // template row offset).
@@ -1287,10 +1327,20 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
       // each lane takes kR consecutive start blocks and every rho
       const int jb = jlo + (sub * 32 + lane) * kR;
+      if (!kAllStarts && Q <= 32) {
+        // the main pass (Q <= 16 here): every lane, the template entries of each
+        // offset held across the lanes, the next offset's loaded ahead
+        R2 tcur = lane < Q ? trow[lane * s] : zero_pair<R2>();
+        for (int rho = 0; rho < s; ++rho) {
+          const R2 tnx = (lane < Q && rho + 1 < s) ? trow[rho + 1 + lane * s] : zero_pair<R2>();
+          correlate_bc<Real, kTwoLevel>(recs, L, min(jb, jhi) * s + rho - k0, s, tcur, Q, acc);
+          tcur = tnx;
+        }
+      }
       if (jb < jhi) {
         if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
           correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
-        } else {
+        } else if (kAllStarts || Q > 32) {
           for (int rho = 0; rho < s; ++rho)
             correlate<Real, kTwoLevel>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
