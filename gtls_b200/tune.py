@@ -1,12 +1,16 @@
 """Autotuning of the search's launch shapes on the caller's own data.
 
-The tile of starts per chi2 CTA and the number of phase buckets of the fold
-ordering change only the time of a search, never its result (every chi2
-value and argmin location is the same; ``tests/test_gpu_tune.py``).  Which
-setting is fastest depends on the curves: the tile against the longest
-duration (halo re-reads versus work per CTA), the bucket count against how
-clustered the folded phases are (regular cadences cluster near multiples of
-the cadence).  ``autotune`` times the main pass of a sample of the trial
+The tile of starts per chi2 CTA, where the chi2 kernel reads the folded
+records from (a shared-memory tile, or global memory through a large L1),
+and the number of phase buckets of the global-scatter fold ordering change
+only the time of a search, never its result (every chi2 value and argmin
+location is the same; ``tests/test_gpu_tune.py``).  Which setting is fastest
+depends on the curves: the tile against the longest duration (halo re-reads
+versus work per CTA; in the FP64 form on a 70,000-sample, 8,400-width curve
+the records read through L1, in tiles of 10,240 starts, beat the staged tile
+by 7.5%), the bucket count against how clustered the folded phases are (it
+matters only for curves above 2^17 samples, which take the global-scatter
+ordering).  ``autotune`` times the main pass of a sample of the trial
 periods under each candidate setting, with the library's own CUDA-event
 stage timing, and keeps the fastest for the context (``gtls_set_tuning``).
 Results are cached per (precision, samples rounded to a power of two,
@@ -18,8 +22,10 @@ import numpy as np
 
 from . import _lib
 
-TILE_CAPS = {"fp32": (8192, 16384, 24576), "fp64": (4096, 8192)}
+TILE_CAPS = {"fp32": (8192, 16384, 24576), "fp64": (4096, 8192, 10240)}
 BUCKET_SHIFTS = (0, -1)
+RECORDS_GLOBAL = (0, 1)
+PACKED_MAX_N = 1 << 17   # curves up to this many samples order their phases in shared memory
 DEFAULT_CAP = {"fp32": 16384, "fp64": 8192}
 MARGIN = 0.02   # a setting must beat the default by this fraction to be chosen
 _CACHE = {}
@@ -30,7 +36,7 @@ def _key(precision, n, maxd):
 
 
 def autotune(run_main_pass, precision, n, maxd, device=0, repeats=2):
-    """Pick the fastest (tile cap, bucket shift) for ``precision``.
+    """Pick the fastest (tile cap, records mode, bucket shift) for ``precision``.
 
     ``run_main_pass(timing)`` runs the main pass of a representative sample
     of periods and fills the ``_lib.Timing`` it is given.  Returns the chosen
@@ -41,9 +47,11 @@ def autotune(run_main_pass, precision, n, maxd, device=0, repeats=2):
     else:
         prev = _lib.get_tuning(device)
         trials = []
-        for cap, shift in itertools.product(TILE_CAPS[precision], BUCKET_SHIFTS):
+        shifts = BUCKET_SHIFTS if n > PACKED_MAX_N else (0,)
+        for cap, rg, shift in itertools.product(TILE_CAPS[precision], RECORDS_GLOBAL, shifts):
             cfg = dict(prev)
             cfg["tile_cap_" + precision] = cap
+            cfg["records_global"] = rg
             cfg["bucket_shift"] = shift
             _lib.set_tuning(device=device, **cfg)
             ms = []
@@ -51,14 +59,14 @@ def autotune(run_main_pass, precision, n, maxd, device=0, repeats=2):
                 tm = _lib.Timing()
                 run_main_pass(tm)
                 ms.append(tm.prepare_ms + tm.chi2_ms + tm.finish_ms)
-            trials.append((min(ms), cap, shift, cfg))
-        trials.sort(key=lambda x: (x[0], x[1], -x[2]))
-        best = trials[0][3]
+            trials.append((min(ms), cap, rg, shift, cfg))
+        trials.sort(key=lambda x: (x[0], x[1], x[2], -x[3]))
+        best = trials[0][4]
         # keep the default unless another setting is clearly faster (timing noise
         # would otherwise make the choice differ from run to run)
-        dflt = [x for x in trials if x[1] == DEFAULT_CAP[precision] and x[2] == 0]
+        dflt = [x for x in trials if x[1] == DEFAULT_CAP[precision] and x[2] == 0 and x[3] == 0]
         if dflt and trials[0][0] > (1.0 - MARGIN) * dflt[0][0]:
-            best = dflt[0][3]
+            best = dflt[0][4]
         _CACHE[key] = best
     _lib.set_tuning(device=device, **best)
     return dict(best)
