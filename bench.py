@@ -8,7 +8,7 @@ finish):
   long-baseline FP64 search -- 70,000 samples at 29.4-min cadence over
   ~1,470 d with 17 gaps, per-sample sigma U(50, 500) ppm + AR(1) red noise,
   one 490 ppm transit at P = 289.9 d; Ofir grid 0.5-735 d at oversampling 3
-  (187,870 periods), 50 durations.  Seeded synthetic data.
+  (187,850 periods), 50 durations.  Seeded synthetic data.
 
 ``value`` is device-timed with the inputs resident in HBM; ``e2e`` times the
 public API from host arrays (host->device copies and result readback inside
@@ -32,7 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "light curves/s (long-baseline TLS search, 70k samples, 187,870 periods x 50 durations)"
+METRIC = "light curves/s (long-baseline TLS search, 70k samples, 187,850 periods x 50 durations)"
 
 
 def parse():
