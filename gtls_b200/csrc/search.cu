@@ -1641,7 +1641,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     long long tile = ((long long)((smem_budget - table) / sizeof(R2)) - maxd - kTilePad) / 256 * 256;
     // records in global memory when the longest duration leaves no room for a
     // shared-memory tile of at least 256 starts (or when the caller asks for it)
-    const bool global_rec = ctx->records_global || tile < 256;
+    // (the all-starts pass keeps the tile: its dense skip-1 sums reuse each
+    // record many times, and it measured faster on the tile)
+    const bool global_rec = (ctx->records_global && !all) || tile < 256;
     if (global_rec) tile = cap;
     tile = std::min<long long>(tile, cap);
     if (tile > n) tile = (n + 255) / 256 * 256;

@@ -95,9 +95,10 @@ typedef struct gtls_tuning {
                                  2^17 samples, and periods whose phases cluster beyond what the
                                  shared-memory ordering holds) = 2^min(15, ceil(log2 N) + shift),
                                  shift in [-3, 0] (0 = default)                               */
-  int32_t records_global;     /* 1: the chi2 kernel reads the folded records from global memory
-                                 (L1/L2) for every curve; 0: from a shared-memory tile when the
-                                 curve's longest duration leaves room for one (default)        */
+  int32_t records_global;     /* 1: the main pass's chi2 kernel reads the folded records from
+                                 global memory (L1/L2) for every curve; 0: from a shared-memory
+                                 tile when the curve's longest duration leaves room for one
+                                 (default).  The all-starts pass always uses the tile when it fits */
 } gtls_tuning;
 
 int gtls_set_tuning(gtls_ctx* ctx, const gtls_tuning* tuning);
