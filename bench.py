@@ -54,7 +54,8 @@ def parse():
                     help="cfg4: one end-to-end gtls_batch call over the sample (e.g. --curves 4096: the whole set), "
                          "after a small warm-up call; wall clock, no timing steps")
     ap.add_argument("--tuning", default=None,
-                    help="fixed launch shapes 'tile_cap_fp32,tile_cap_fp64,bucket_shift' instead of autotuning "
+                    help="fixed launch shapes 'tile_cap_fp32,tile_cap_fp64,bucket_shift[,records_global]' instead of "
+                         "autotuning "
                          "(profiling runs: ncu slows untimed launches, which would skew the tuner)")
     ap.add_argument("--chunk-mb", type=int, default=0,
                     help="per-chunk scratch budget of the searches in MiB (default: the library's 8 GiB)")
@@ -395,8 +396,10 @@ def fixed_or_tuned(args, tune_fn, device):
     the device's context and returns them."""
     from gtls_b200 import _lib
     if args.tuning:
-        c32, c64, shift = (int(v) for v in args.tuning.split(","))
-        _lib.set_tuning(tile_cap_fp32=c32, tile_cap_fp64=c64, bucket_shift=shift, device=device)
+        vals = [int(v) for v in args.tuning.split(",")]
+        c32, c64, shift = vals[:3]
+        rg = vals[3] if len(vals) > 3 else 0
+        _lib.set_tuning(tile_cap_fp32=c32, tile_cap_fp64=c64, bucket_shift=shift, records_global=rg, device=device)
         return _lib.get_tuning(device)
     return tune_fn()
 
