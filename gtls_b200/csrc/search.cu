@@ -137,6 +137,8 @@ struct CurveDev {
   int tile, ntiles, nb_log2;
   int rnb_log2, rcap;           // shared-memory prepare path: bucket bits and round capacity (0: off)
   int global_rec;               // 1: chi2 reads the records from global memory (no shared tile)
+  int maxd_l;                   // > 0 (global records, main pass): the lane path's records, the tile
+                                // plus this halo (its longest width), are staged in shared memory
   float span;
 };
 
@@ -1060,7 +1062,13 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   const int* __restrict__ skips = C.skips;
   const int lane = threadIdx.x & 31;
   // per-duration table after the tile: overshoot, (width | skip << 16), template row offset
-  Real* dtab_os = reinterpret_cast<Real*>(smem_raw + (kGlobal ? 0 : chi2_tile_bytes<Real>(C.tile, C.maxd)));
+  // staged records: the whole tile and halo, or (global records) only what
+  // the lane path reads, when the host made room for it
+  const bool stage = !kGlobal || C.maxd_l > 0;
+  const int Lt = kGlobal ? (k1 - k0) + C.maxd_l - 1 : L;
+  Real* dtab_os = reinterpret_cast<Real*>(
+      smem_raw + (kGlobal ? (C.maxd_l > 0 ? chi2_tile_bytes<Real>(C.tile, C.maxd_l) : 0)
+                          : chi2_tile_bytes<Real>(C.tile, C.maxd)));
   int* dtab_ws = reinterpret_cast<int*>(dtab_os + D);
   int* dtab_row = dtab_ws + D;
   const R2* __restrict__ trows = C.trows;
@@ -1073,8 +1081,8 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
 
   // stage the records [k0, k0 + L) in shared memory with one bulk (TMA) copy;
   // the byte count is rounded up to 16 (the record rows are padded for it)
-  const uint32_t tile_bytes = (uint32_t)(((size_t)L * sizeof(R2) + 15) & ~(size_t)15);
-  if (!kGlobal && threadIdx.x == 0) {
+  const uint32_t tile_bytes = (uint32_t)(((size_t)Lt * sizeof(R2) + 15) & ~(size_t)15);
+  if (stage && threadIdx.x == 0) {
     mbar_init(&tile_bar, 1);
     mbar_arrive_expect_tx(&tile_bar, tile_bytes);
     bulk_g2s(tile, src, tile_bytes, &tile_bar);
@@ -1111,7 +1119,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       task_pre[ucnt] = carry;
       task_next = 0;
       work_sm[0] = work_sm[1] = 0;
-      if constexpr (kGlobal) {
+      if (!stage) {
         tile_ok = 1;
       } else {
         tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
@@ -1127,10 +1135,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     }
   }
   __syncthreads();
-  if constexpr (!kGlobal) {
-    // zero the pad after the tile's L records (the copy's rounding to 16 bytes
+  if (stage) {
+    // zero the pad after the tile's Lt records (the copy's rounding to 16 bytes
     // may have brought in one record past them, possibly an unwritten one)
-    for (int i = L + (int)threadIdx.x; i < L + kTilePad; i += blockDim.x) {
+    for (int i = Lt + (int)threadIdx.x; i < Lt + kTilePad; i += blockDim.x) {
       R2 zr;
       zr.x = (Real)0;
       zr.y = (Real)0;
@@ -1139,6 +1147,8 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   }
   __syncthreads();
   const R2* recs = kGlobal ? src : tile;   // the records [k0, k0 + L)
+  const R2* recl = stage ? tile : src;     // the lane path's: [k0, k0 + Ll)
+  const int Ll = stage ? Lt : L;
 
   Best best{INFINITY, 0x7fffffffffffffffLL};
   // the first start skipped by k % skip != 0 carries the value n (GPUFun.py:407,409)
@@ -1284,10 +1294,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
         for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
         if (jb < jhi) {
           if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
-            correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
+            correlate_s1<Real, kTwoLevel>(recl, jb - k0, trow, Qr, acc);
           } else {
             for (int rho = 0; rho < s; ++rho)
-              correlate<Real, kTwoLevel>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+              correlate<Real, kTwoLevel>(recl, Ll, jb * s + rho - k0, s, trow, rho, Q, acc);
           }
           Pv p0[kR], pw[kR];
 #pragma unroll
@@ -1333,16 +1343,16 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
         R2 tcur = lane < Q ? trow[lane * s] : zero_pair<R2>();
         for (int rho = 0; rho < s; ++rho) {
           const R2 tnx = (lane < Q && rho + 1 < s) ? trow[rho + 1 + lane * s] : zero_pair<R2>();
-          correlate_bc<Real, kTwoLevel>(recs, L, min(jb, jhi) * s + rho - k0, s, tcur, Q, acc);
+          correlate_bc<Real, kTwoLevel>(recl, Ll, min(jb, jhi) * s + rho - k0, s, tcur, Q, acc);
           tcur = tnx;
         }
       }
       if (jb < jhi) {
         if (kAllStarts && !kGlobal && s == 1 && jb + kR <= jhi) {
-          correlate_s1<Real, kTwoLevel>(recs, jb - k0, trow, Qr, acc);
+          correlate_s1<Real, kTwoLevel>(recl, jb - k0, trow, Qr, acc);
         } else if (kAllStarts || Q > 32) {
           for (int rho = 0; rho < s; ++rho)
-            correlate<Real, kTwoLevel>(recs, L, jb * s + rho - k0, s, trow, rho, Q, acc);
+            correlate<Real, kTwoLevel>(recl, Ll, jb * s + rho - k0, s, trow, rho, Q, acc);
         }
         // the prefix values of the lane's kR starts, all loads in flight
         // together (indices clamped to the last start of the tile; values of
@@ -1670,6 +1680,13 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     C.nb_log2 = nb_log2_for(n, ctx->bucket_shift);
     rounds_params(C, ctx->smem_optin);
     C.global_rec = global_rec ? 1 : 0;
+    C.maxd_l = 0;
+    if (global_rec && !all) {
+      int mx = 0;
+      for (int i = 0; i < D; ++i)
+        if (hskip[c][i] < kSplitMinSkip) mx = std::max(mx, hw[c][i]);
+      if (mx > 0 && chi2_smem_bytes<Real>((int)tile, mx, D) <= smem_budget) C.maxd_l = mx;
+    }
     C.span = h.span;
     p_off[c + 1] = p_off[c] + h.np;
     b_off[c + 1] = b_off[c] + C.nbatch;
@@ -1773,7 +1790,8 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
         items += (int)take;
         tiles += (int)(take * C.ntiles);
         sm_prep = std::max(sm_prep, prep_smem_bytes(C));
-        sm_chi = std::max(sm_chi, C.global_rec ? (size_t)C.D * (sizeof(Real) + 2 * sizeof(int))
+        sm_chi = std::max(sm_chi, C.global_rec ? (C.maxd_l > 0 ? chi2_smem_bytes<Real>(C.tile, C.maxd_l, C.D)
+                                                                : (size_t)C.D * (sizeof(Real) + 2 * sizeof(int)))
                                                : chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
         mode = C.global_rec;
         p += take;
