@@ -1119,8 +1119,8 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       task_pre[ucnt] = carry;
       task_next = 0;
       work_sm[0] = work_sm[1] = 0;
-      if (!stage) {
-        tile_ok = 1;
+      if (!stage || kGlobal) {
+        tile_ok = 1;   // global records: the warps that need the lane path's tile wait for it
       } else {
         tile_ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
         if (!tile_ok) {
@@ -1135,7 +1135,7 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
     }
   }
   __syncthreads();
-  if (stage) {
+  if (stage && !kGlobal) {
     // zero the pad after the tile's Lt records (the copy's rounding to 16 bytes
     // may have brought in one record past them, possibly an unwritten one)
     for (int i = Lt + (int)threadIdx.x; i < Lt + kTilePad; i += blockDim.x) {
@@ -1161,6 +1161,10 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
   }
   const int ntask = tile_ok ? task_pre[ucnt] : 0;
   const bool count_work = a.work != nullptr;
+  // global records with a staged lane-path tile: the split path starts at
+  // once; a warp waits for the tile (bounded) before its first lane-path task
+  bool lane_tile = !(kGlobal && stage);
+  bool lane_skip = false;
   while (true) {
     int tk = 0;
     if (lane == 0) tk = atomicAdd(&task_next, 1);
@@ -1333,6 +1337,22 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
         if (lane == 0) atomicAdd(&work_sm[0], (unsigned long long)nact * 2ULL * (unsigned)w);
       }
     } else {
+      if constexpr (kGlobal) {
+        if (!lane_tile) {
+          int ok = 1;
+          if (lane == 0) {
+            ok = mbar_wait_bounded(&tile_bar, 0, 1LL << 22) ? 1 : 0;
+            if (!ok) atomicOr(a.status, 1);
+          }
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          lane_skip = !ok;
+          if (ok)
+            for (int i = Lt + lane; i < Lt + kTilePad; i += 32) tile[i] = zero_pair<R2>();
+          __syncwarp();
+          lane_tile = true;
+        }
+        if (lane_skip) continue;   // the status word reports it
+      }
 #pragma unroll
       for (int r = 0; r < kR; ++r) acc[r] = zero_pair<R2>();
       // each lane takes kR consecutive start blocks and every rho
@@ -1391,6 +1411,8 @@ chi2_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs
       }
     }
   }
+  // a staged copy that no warp waited for must land before the CTA exits
+  if (kGlobal && stage && threadIdx.x == 0) mbar_wait_bounded(&tile_bar, 0, 1LL << 26);
   // CTA minimum (value, then location)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 
-TILE_CAPS = {"fp32": (8192, 12288, 16384, 24576), "fp64": (4096, 8192, 10240)}
+TILE_CAPS = {"fp32": (8192, 12288, 16384, 24576), "fp64": (4096, 8192, 10240, 12288)}
 BUCKET_SHIFTS = (0, -1)
 RECORDS_GLOBAL = (0, 1)
 PACKED_MAX_N = 1 << 17   # curves up to this many samples order their phases in shared memory
