@@ -52,6 +52,8 @@
 namespace gtls {
 
 constexpr int kPrepThreads = 1024;
+constexpr int kPrepThreadsSmall = 512;   // curves of at most kPrepSmallMaxN samples: two CTAs per SM
+constexpr int kPrepSmallMaxN = 1 << 15;
 constexpr int kSmallBucket = 8;     // entries of buckets up to this size are ranked by their own thread
 constexpr int kSmallBucketSm = 16;  // the same, for buckets in shared memory
 constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (warp-ranked)
@@ -660,9 +662,12 @@ __device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum,
 
 // kOrder: write only the stable fold order of each period (order_out[rec_off
 // + local * n + p] = original index of sorted position p) instead of the
-// records and prefix (gtls_fold_order).
-template <typename Real, bool kOrder = false>
-__global__ void __launch_bounds__(kPrepThreads)
+// records and prefix (gtls_fold_order).  kThreads: kPrepThreads (one CTA per
+// SM), or kPrepThreadsSmall for curves of at most kPrepSmallMaxN samples
+// (two CTAs per SM, each with half the shared memory: the barriers of one
+// overlap the other's work, which pays on short curves).
+template <typename Real, bool kOrder = false, int kThreads = kPrepThreads>
+__global__ void __launch_bounds__(kThreads, kPrepThreads / kThreads)
 prepare_kernel(const CurveDev<Real>* __restrict__ cds, const Run* __restrict__ runs, int nruns,
                uint2* __restrict__ scr_slot, typename Tr<Real>::R2* __restrict__ rec,
                typename Tr<Real>::Pv* __restrict__ pv, int* __restrict__ order_out = nullptr) {
@@ -1578,7 +1583,8 @@ __global__ void template_rows_kernel(const CurveDev<Real>* __restrict__ cds, con
 static int nb_log2_for(int n, int shift) {
   int k = 1;
   while ((1 << k) < n) ++k;
-  k = std::min(15, k + shift);   // at most 32768 buckets (128 KB of counters)
+  // at most 32768 buckets (128 KB of counters), 16384 in the two-per-SM shape
+  k = std::min(n <= kPrepSmallMaxN ? 14 : 15, k + shift);
   return std::max(1, k);
 }
 
@@ -1598,7 +1604,9 @@ static void rounds_params(CurveDev<Real>& C, int smem_optin) {
   int k = 1;
   while ((1 << k) < n) ++k;
   const int nbl = std::max(1, std::min(14, k - 2));
-  const long long c = std::min<long long>(((long long)smem_optin - kPrepStaticSmem - (4LL << nbl)) / 16, n);
+  // two CTAs per SM for short curves: each gets half the shared memory
+  const long long budget = (n <= kPrepSmallMaxN ? smem_optin / 2 : smem_optin) - kPrepStaticSmem;
+  const long long c = std::min<long long>((budget - (4LL << nbl)) / 16, n);
   if (c < 1024 && c < n) return;
   C.rnb_log2 = nbl;
   C.rcap = (int)c;
@@ -1754,6 +1762,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
   std::vector<int> chunk_r0, chunk_items, chunk_tiles;
   std::vector<size_t> chunk_smem_prep, chunk_smem_chi;
   std::vector<int> chunk_global;   // per chunk: records of all its curves in global memory (1) or tiles (0)
+  std::vector<int> chunk_small;    // per chunk: all its curves take the two-per-SM prepare shape
   size_t max_slot = 0, max_rec = 0, max_pv = 0, max_part = 0;
   {
     size_t slot = 0, rec = 0, pvs = 0, bytes = 0;
@@ -1763,7 +1772,8 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     chunk_r0.push_back(0);
     auto close_chunk = [&]() {
       if (items == 0) return;
-      chunk_global.push_back(mode);
+      chunk_global.push_back(mode & 1);
+      chunk_small.push_back(mode >> 1);
       chunk_items.push_back(items);
       chunk_tiles.push_back(tiles);
       chunk_smem_prep.push_back(sm_prep);
@@ -1783,7 +1793,9 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
       const size_t per = (size_t)C.n * 8 + (size_t)C.Mrec * sizeof(R2) + (size_t)(C.M + 1) * sizeof(Pv) +
                          (size_t)C.ntiles * 16;
       long long p = 0;
-      if (C.np > 0 && mode != -1 && mode != C.global_rec) close_chunk();   // one records mode per chunk
+      // one records mode and one prepare shape per chunk
+      const int cmode = C.global_rec | (C.n <= kPrepSmallMaxN ? 2 : 0);
+      if (C.np > 0 && mode != -1 && mode != cmode) close_chunk();
       while (p < C.np) {
         long long fit = (long long)((budget > bytes ? budget - bytes : 0) / per);
         fit = std::min<long long>(fit, (long long)INT32_MAX - items);
@@ -1815,7 +1827,7 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
         sm_chi = std::max(sm_chi, C.global_rec ? (C.maxd_l > 0 ? chi2_smem_bytes<Real>(C.tile, C.maxd_l, C.D)
                                                                 : (size_t)C.D * (sizeof(Real) + 2 * sizeof(int)))
                                                : chi2_smem_bytes<Real>(C.tile, C.maxd, C.D));
-        mode = C.global_rec;
+        mode = cmode;
         p += take;
       }
     }
@@ -1914,6 +1926,8 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
     max_prep = std::max(max_prep, chunk_smem_prep[k]);
     max_chi = std::max(max_chi, chunk_smem_chi[k]);
   }
+  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<Real, false, kPrepThreadsSmall>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(max_prep, 1)));
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)std::max<size_t>(max_prep, 1)));
   GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(chi2_kernel<Real, false, false>,
@@ -1939,7 +1953,11 @@ static int run_search(gtls_ctx* ctx, const CurveHost* ch, int n_curves, int prec
       for (auto& e : e3) GTLS_TRY_CUDA(ctx, cudaEventCreate(&e));
       GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[0], st));
     }
-    prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, rec, pv);
+    if (chunk_small[k])
+      prepare_kernel<Real, false, kPrepThreadsSmall><<<items, kPrepThreadsSmall, chunk_smem_prep[k], st>>>(
+          d_cd, d_runs + r0, nr, scr_slot, rec, pv);
+    else
+      prepare_kernel<Real><<<items, kPrepThreads, chunk_smem_prep[k], st>>>(d_cd, d_runs + r0, nr, scr_slot, rec, pv);
     if (tm) GTLS_TRY_CUDA(ctx, cudaEventRecord(e3[1], st));
     ca.nruns = nr;
     using ChiKernel = void (*)(const CurveDev<Real>*, const Run*, const R2*, const Pv*, Chi2Args);
@@ -2151,11 +2169,18 @@ extern "C" int gtls_fold_order(gtls_ctx* ctx, const double* t, int32_t n, const 
   GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_cd, &C, sizeof(C), cudaMemcpyHostToDevice, st));
   GTLS_TRY_CUDA(ctx, cudaMemcpyAsync(d_runs, runs.data(), sizeof(Run) * runs.size(), cudaMemcpyHostToDevice, st));
   const size_t smem = prep_smem_bytes(C);
-  GTLS_TRY_CUDA(ctx, cudaFuncSetAttribute(prepare_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+  const bool small = n <= kPrepSmallMaxN;
+  GTLS_TRY_CUDA(ctx, small ? cudaFuncSetAttribute(prepare_kernel<double, true, kPrepThreadsSmall>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(prepare_kernel<double, true>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (size_t k = 0; k < runs.size(); ++k) {
-    prepare_kernel<double, true><<<runs[k].count, kPrepThreads, smem, st>>>(d_cd, d_runs + k, 1, slots, nullptr,
-                                                                             nullptr, order_out);
+    if (small)
+      prepare_kernel<double, true, kPrepThreadsSmall><<<runs[k].count, kPrepThreadsSmall, smem, st>>>(
+          d_cd, d_runs + k, 1, slots, nullptr, nullptr, order_out);
+    else
+      prepare_kernel<double, true><<<runs[k].count, kPrepThreads, smem, st>>>(d_cd, d_runs + k, 1, slots, nullptr,
+                                                                               nullptr, order_out);
     ctx->launches += 1;
     GTLS_TRY_CUDA(ctx, cudaGetLastError());
   }
