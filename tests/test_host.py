@@ -350,3 +350,46 @@ def test_cfg3_oracle_fixture_matches_the_product_grid():
         sc = f["seed%d_scalars" % seed]
         assert len(f["seed%d_chi2" % seed]) == len(P)
         assert P[int(sc[0])] == sc[1]
+
+
+def test_autotune_sweep_and_choice(monkeypatch):
+    """The tuner's sweep and choice, with the library replaced by a fake
+    tuning store and made-up stage times: records mode and tile cap are
+    swept for every curve, the bucket shift only above 2^17 samples (where
+    the global-scatter ordering runs); the default stays unless another
+    setting is faster by the margin."""
+    from gtls_b200 import _lib, tune
+
+    state = dict(tile_cap_fp32=16384, tile_cap_fp64=8192, bucket_shift=0, records_global=0)
+    seen = []
+
+    def set_tuning(device=0, **cfg):
+        state.update(cfg)
+
+    monkeypatch.setattr(_lib, "get_tuning", lambda device=0: dict(state))
+    monkeypatch.setattr(_lib, "set_tuning", set_tuning)
+
+    def make_run(times):
+        def run(tm):
+            key = (state["tile_cap_fp64"], state["records_global"], state["bucket_shift"])
+            seen.append(key)
+            tm.prepare_ms, tm.chi2_ms, tm.finish_ms = 1.0, times.get(key, 10.0), 0.0
+        return run
+
+    # a clearly faster global-records setting is chosen
+    tune._CACHE.clear()
+    best = tune.autotune(make_run({(10240, 1, 0): 8.0}), "fp64", n=70000, maxd=8400)
+    assert (best["tile_cap_fp64"], best["records_global"]) == (10240, 1)
+    assert {k[2] for k in seen} == {0}                      # no bucket sweep at 70,000 samples
+    assert {(k[0], k[1]) for k in seen} == {(c, r) for c in tune.TILE_CAPS["fp64"] for r in (0, 1)}
+    # within the margin the default is kept
+    seen.clear()
+    tune._CACHE.clear()
+    best = tune.autotune(make_run({(10240, 1, 0): 9.9}), "fp64", n=70000, maxd=8400)
+    assert (best["tile_cap_fp64"], best["records_global"], best["bucket_shift"]) == (8192, 0, 0)
+    # above 2^17 samples the bucket shift is swept too
+    seen.clear()
+    tune._CACHE.clear()
+    tune.autotune(make_run({}), "fp64", n=200000, maxd=8400)
+    assert {k[2] for k in seen} == set(tune.BUCKET_SHIFTS)
+    tune._CACHE.clear()
