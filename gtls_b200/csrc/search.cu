@@ -67,7 +67,7 @@ constexpr int kSplitMinSkip = 32;  // skip >= this: lanes split the block offset
 // starts are first put through the depth test; the starts that pass are then
 // covered by groups of kR consecutive starts (each beginning at the first
 // uncovered start that passes), and only those groups are correlated.
-constexpr int kWin = 4 * kR;
+constexpr int kWin = 6 * kR;
 // All-starts pass, lane-path task of a width of at least kLaneGateMinW: a
 // window of 32 * kLaneG groups of kR consecutive starts; the groups whose
 // starts all fail the depth test are dropped and the others are dealt out to
