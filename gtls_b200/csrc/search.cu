@@ -55,7 +55,7 @@ constexpr int kPrepThreads = 1024;
 constexpr int kPrepThreadsSmall = 512;   // curves of at most kPrepSmallMaxN samples: two CTAs per SM
 constexpr int kPrepSmallMaxN = 1 << 15;
 constexpr int kSmallBucket = 8;     // entries of buckets up to this size are ranked by their own thread
-constexpr int kSmallBucketSm = 16;  // the same, for buckets in shared memory
+constexpr int kSmallBucketSm = 32;  // the same, for buckets in shared memory
 constexpr int kBigBuckets = 512;    // capacity of the list of larger buckets (warp-ranked)
 constexpr int kMaxRounds = 32;      // rounds of the shared-memory prepare path
 constexpr int kRoundShift = 20;     // hist entries of that path: position | round << kRoundShift
@@ -424,7 +424,7 @@ __device__ __noinline__ bool prepare_rounds(int* dyn, int* wtmp_i, double* wsum,
   uint2* slots = reinterpret_cast<uint2*>(dyn + nb);
   double* vbuf = reinterpret_cast<double*>(slots + cap);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  constexpr int kB = 4;   // elements per thread in flight in each pass
+  constexpr int kB = 2;   // elements per thread in flight in each pass (4 and 8 measured slower)
   const int stride = blockDim.x * kB;
 
   for (int b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
