@@ -74,7 +74,7 @@ constexpr int kWin = 6 * kR;
 // the lanes round by round.  (For shorter widths, and for the main pass's
 // lane-path widths, measured: a group's sums cost about what its depth tests
 // do, and the task is the plain 32 groups.)
-constexpr int kLaneG = 4;
+constexpr int kLaneG = 6;            // (2 and 4 measured slower)
 constexpr int kLaneGateMinW = 64;
 // Zeroed records after each shared-memory tile: a skip-1 group whose kR
 // starts all lie in the tile reads at most kR - 2 records past it (only ever
